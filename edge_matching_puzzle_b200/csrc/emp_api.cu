@@ -1,0 +1,464 @@
+// C ABI of edge_matching_puzzle_b200 (include/emp_b200.h): puzzle handles and
+// the exhaustive backtracker.
+#include "emp_b200.h"
+#include "emp_bt.h"
+#include "emp_common.h"
+#include "emp_model.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cstring>
+#include <memory>
+#include <new>
+#include <string>
+#include <vector>
+
+using emp::DeviceBuffer;
+using emp::fail;
+
+extern "C" uint32_t emp_abi_version(void) { return EMP_ABI_VERSION; }
+
+extern "C" const char* emp_last_error(void) { return emp::last_error().c_str(); }
+
+extern "C" emp_status emp_generate_puzzle(uint32_t width, uint32_t height, uint32_t border_colors,
+                                          uint32_t interior_colors, uint64_t seed, uint8_t* colours_out)
+{
+    emp::clear_error();
+    if (!colours_out || width < 2 || height < 2 || width * height > emp::kMaxPieces)
+        return fail(EMP_ERR_INVALID, "emp_generate_puzzle: need 2<=w,h, w*h<=256 and an output buffer");
+    if (border_colors < 1 || interior_colors < 1 || border_colors + interior_colors + 1 > emp::kMaxColourId)
+        return fail(EMP_ERR_INVALID, "emp_generate_puzzle: colour counts out of range");
+    emp::generate_puzzle(width, height, border_colors, interior_colors, seed, colours_out);
+    return EMP_OK;
+}
+
+extern "C" emp_status emp_puzzle_create(const emp_puzzle_desc* desc, emp_puzzle* out)
+{
+    emp::clear_error();
+    if (!desc || !out || !desc->colours) return fail(EMP_ERR_INVALID, "emp_puzzle_create: null argument");
+    *out = nullptr;
+    std::unique_ptr<emp_puzzle_t> p(new (std::nothrow) emp_puzzle_t());
+    if (!p) return fail(EMP_ERR_NOMEM, "emp_puzzle_create: out of host memory");
+    std::string err;
+    if (desc->width * desc->height > emp::kMaxPieces)
+        return fail(EMP_ERR_UNSUPPORTED, "emp_puzzle_create: more than 256 pieces");
+    if (!emp::build_model(desc->width, desc->height, desc->colours, p->model, err))
+        return fail(err.find("colour ids above") != std::string::npos ? EMP_ERR_UNSUPPORTED : EMP_ERR_INVALID,
+                    "emp_puzzle_create: " + err);
+    const uint32_t n = p->model.n;
+    if (desc->order) p->order.assign(desc->order, desc->order + n);
+    else p->order = emp::order_basic(desc->width, desc->height);
+    if (!emp::build_plan(p->model, p->order, p->plan, err)) return fail(EMP_ERR_INVALID, "emp_puzzle_create: " + err);
+    emp::build_device_tables(p->model, p->plan, p->tables);
+    for (uint32_t k = 0; k < 3; ++k)
+        for (uint32_t e = 0; e < 4 * p->model.nb_kind(k); ++e)
+            p->extra_count += (p->tables.blob[p->tables.tinfo_kind_off[k] + e] >> 20) & 1u;
+    *out = p.release();
+    return EMP_OK;
+}
+
+extern "C" void emp_puzzle_destroy(emp_puzzle puzzle) { delete puzzle; }
+
+extern "C" emp_status emp_puzzle_get_info(emp_puzzle p, emp_puzzle_info* info)
+{
+    emp::clear_error();
+    if (!p || !info) return fail(EMP_ERR_INVALID, "emp_puzzle_get_info: null argument");
+    info->width = p->model.width;
+    info->height = p->model.height;
+    info->nb_pieces = p->model.n;
+    info->nb_center = p->model.nb_kind(0);
+    info->nb_border = p->model.nb_kind(1);
+    info->nb_corner = p->model.nb_kind(2);
+    info->border_color_id = p->model.border_id;
+    info->has_identical = p->model.has_identical ? 1u : 0u;
+    info->identical_masks_with_extra = p->extra_count;
+    return EMP_OK;
+}
+
+extern "C" emp_status emp_puzzle_export_tables(emp_puzzle p, uint32_t* out, uint64_t capacity, uint64_t* words)
+{
+    emp::clear_error();
+    if (!p || !words) return fail(EMP_ERR_INVALID, "emp_puzzle_export_tables: null argument");
+    *words = p->tables.blob.size();
+    if (out && capacity >= p->tables.blob.size())
+        std::memcpy(out, p->tables.blob.data(), sizeof(uint32_t) * p->tables.blob.size());
+    return EMP_OK;
+}
+
+// ---------------------------------------------------------------------------
+// exhaustive backtracker plans
+
+struct emp_bt_plan_t {
+    std::vector<emp_puzzle> puzzles;
+    emp_bt_config cfg{};
+    int device = 0;
+    uint32_t depth = 0, max_levels = 0, max_avail = 0, max_kw = 0;
+    uint32_t threads = 128, blocks = 0, rec_words = 0;
+    uint64_t capacity = 0, budget = 0;
+    DeviceBuffer tables, poff;
+    DeviceBuffer prefixes, prefix_puzzle;     // split-depth prefixes (all)
+    DeviceBuffer rec_init, rec_a, rec_b;      // initial records (selection), round queues
+    DeviceBuffer counters;                    // [0] cursor, [1] output tail
+    DeviceBuffer totals, first_item, records, flags, item_nodes, item_sols, spill, prefix_out;
+    uint64_t n_all = 0, n_init = 0;
+    bool sampled = false;
+    std::vector<unsigned long long> exp_nodes, exp_sols;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    bool ran = false;
+    uint32_t rounds = 0;
+
+    ~emp_bt_plan_t()
+    {
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+    }
+
+    emp::BtLaunch launch() const
+    {
+        emp::BtLaunch P;
+        P.tables = tables.as<uint32_t>();
+        P.puzzle_offset = poff.as<uint64_t>();
+        P.depth = depth;
+        P.max_levels = max_levels;
+        P.max_avail_words = max_avail;
+        P.max_kw = max_kw;
+        P.spill = spill.as<uint32_t>();
+        P.rec_words = rec_words;
+        P.rec_r_off = rec_words - max_kw;
+        P.out_capacity = capacity;
+        P.item_budget = budget;
+        unsigned long long* c = counters.as<unsigned long long>();
+        P.cursor = c;
+        P.out_tail = c + 1;
+        P.totals = totals.as<unsigned long long>();
+        P.item_nodes = item_nodes.as<unsigned long long>();
+        P.item_sols = item_sols.as<unsigned long long>();
+        P.first_item = first_item.as<unsigned long long>();
+        P.first_records = records.as<emp::FirstRecord>();
+        P.timeout_ns = static_cast<unsigned long long>(cfg.timeout_ms) * 1000000ull;
+        P.abort_flag = flags.as<int>();
+        P.status = flags.as<int>() + 1;
+        P.stop_at_first = cfg.stop_at_first ? 1 : 0;
+        return P;
+    }
+};
+
+namespace {
+
+uint32_t auto_depth(uint32_t min_n)
+{
+    // Deep enough to give every resident thread several subtrees on the
+    // project's 8x8 workloads, never the last level.
+    const uint32_t d = min_n >= 36 ? 12 : min_n / 2;
+    return std::max<uint32_t>(1, std::min<uint32_t>(d, min_n - 1));
+}
+
+emp_status expand(emp_bt_plan_t& pl)
+{
+    const uint32_t P = static_cast<uint32_t>(pl.puzzles.size());
+    cudaStream_t st = nullptr;
+    emp::BtLaunch L = pl.launch();
+    DeviceBuffer parents, parent_puzzle, children, child_puzzle, counts, offsets, bsums, grand, lv;
+    CUDA_TRY(lv.alloc(sizeof(unsigned long long) * 2 * P));
+    CUDA_TRY(cudaMemsetAsync(lv.p, 0, lv.bytes, st));
+    CUDA_TRY(parent_puzzle.alloc(sizeof(uint32_t) * P));
+    {
+        std::vector<uint32_t> ids(P);
+        for (uint32_t i = 0; i < P; ++i) ids[i] = i;
+        CUDA_TRY(cudaMemcpyAsync(parent_puzzle.p, ids.data(), sizeof(uint32_t) * P, cudaMemcpyHostToDevice, st));
+    }
+    CUDA_TRY(parents.alloc(2));
+    CUDA_TRY(grand.alloc(sizeof(uint64_t)));
+    uint64_t np = P;
+    unsigned long long* lnodes = lv.as<unsigned long long>();
+    for (uint32_t level = 0; level < pl.depth; ++level) {
+        CUDA_TRY(counts.alloc(sizeof(uint32_t) * std::max<uint64_t>(np, 1)));
+        CUDA_TRY(offsets.alloc(sizeof(uint64_t) * std::max<uint64_t>(np, 1)));
+        CUDA_TRY(bsums.alloc(sizeof(uint64_t) * emp::scan_block_sum_words(np)));
+        CUDA_TRY(emp::launch_expand(L, parents.as<uint16_t>(), parent_puzzle.as<uint32_t>(), np, level,
+                                    counts.as<uint32_t>(), nullptr, nullptr, nullptr, lnodes, lnodes + P, 0, st));
+        CUDA_TRY(emp::launch_scan(counts.as<uint32_t>(), np, offsets.as<uint64_t>(), bsums.as<uint64_t>(),
+                                  grand.as<uint64_t>(), st));
+        uint64_t total = 0;
+        CUDA_TRY(cudaMemcpyAsync(&total, grand.p, sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
+        CUDA_TRY(cudaStreamSynchronize(st));
+        CUDA_TRY(children.alloc(sizeof(uint16_t) * std::max<uint64_t>(total, 1) * (level + 1)));
+        CUDA_TRY(child_puzzle.alloc(sizeof(uint32_t) * std::max<uint64_t>(total, 1)));
+        CUDA_TRY(emp::launch_expand(L, parents.as<uint16_t>(), parent_puzzle.as<uint32_t>(), np, level,
+                                    counts.as<uint32_t>(), offsets.as<uint64_t>(), children.as<uint16_t>(),
+                                    child_puzzle.as<uint32_t>(), lnodes, lnodes + P, 1, st));
+        std::swap(parents, children);
+        std::swap(parent_puzzle, child_puzzle);
+        np = total;
+        if (!np) break;
+    }
+    pl.exp_nodes.assign(P, 0);
+    pl.exp_sols.assign(P, 0);
+    CUDA_TRY(cudaMemcpyAsync(pl.exp_nodes.data(), lnodes, sizeof(unsigned long long) * P, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaMemcpyAsync(pl.exp_sols.data(), lnodes + P, sizeof(unsigned long long) * P, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    pl.n_all = np;
+    pl.prefixes = std::move(parents);
+    pl.prefix_puzzle = std::move(parent_puzzle);
+    return EMP_OK;
+}
+
+// Initial records for subtrees first, first+stride, ... (count of them).
+emp_status build_initial(emp_bt_plan_t& pl, uint64_t first, uint64_t stride, uint64_t count)
+{
+    CUDA_TRY(pl.rec_init.alloc(sizeof(uint32_t) * pl.rec_words * std::max<uint64_t>(count, 1)));
+    CUDA_TRY(emp::launch_make_records(pl.prefixes.as<uint16_t>(), pl.prefix_puzzle.as<uint32_t>(), pl.depth, first,
+                                      stride, count, pl.rec_words, pl.rec_init.as<uint32_t>(), nullptr));
+    if (pl.cfg.keep_subtree_counts) {
+        CUDA_TRY(pl.item_nodes.alloc(sizeof(unsigned long long) * std::max<uint64_t>(count, 1)));
+        CUDA_TRY(pl.item_sols.alloc(sizeof(unsigned long long) * std::max<uint64_t>(count, 1)));
+    }
+    CUDA_TRY(cudaDeviceSynchronize());
+    pl.n_init = count;
+    return EMP_OK;
+}
+
+}  // namespace
+
+extern "C" emp_status emp_bt_plan_create(const emp_puzzle* puzzles, uint32_t count, const emp_bt_config* config,
+                                         emp_bt_plan* out)
+{
+    emp::clear_error();
+    if (!puzzles || !count || !out) return fail(EMP_ERR_INVALID, "emp_bt_plan_create: no puzzle");
+    if (count > 65535) return fail(EMP_ERR_UNSUPPORTED, "emp_bt_plan_create: at most 65535 puzzles per plan");
+    *out = nullptr;
+    std::unique_ptr<emp_bt_plan_t> pl(new (std::nothrow) emp_bt_plan_t());
+    if (!pl) return fail(EMP_ERR_NOMEM, "emp_bt_plan_create: out of host memory");
+    if (config) pl->cfg = *config;
+    else pl->cfg.device = -1;
+    uint32_t min_n = ~0u;
+    for (uint32_t i = 0; i < count; ++i) {
+        if (!puzzles[i]) return fail(EMP_ERR_INVALID, "emp_bt_plan_create: null puzzle");
+        pl->puzzles.push_back(puzzles[i]);
+        const emp::DeviceTables& t = puzzles[i]->tables;
+        min_n = std::min(min_n, t.n);
+        pl->max_levels = std::max(pl->max_levels, t.n);
+        pl->max_avail = std::max(pl->max_avail, t.avail_words);
+        for (uint32_t k = 0; k < 3; ++k) pl->max_kw = std::max(pl->max_kw, t.kw[k]);
+    }
+    pl->depth = pl->cfg.split_depth ? pl->cfg.split_depth : auto_depth(min_n);
+    if (pl->depth >= min_n || pl->depth > 64)
+        return fail(EMP_ERR_INVALID, "emp_bt_plan_create: split depth must be below the piece count and at most 64");
+    pl->rec_words = emp::record_words(pl->max_levels, pl->max_kw);
+    EMP_TRY(emp::select_device(pl->cfg.device, &pl->device));
+    // tables
+    std::vector<uint32_t> blob;
+    std::vector<uint64_t> offs;
+    for (emp_puzzle p : pl->puzzles) {
+        offs.push_back(blob.size());
+        blob.insert(blob.end(), p->tables.blob.begin(), p->tables.blob.end());
+    }
+    CUDA_TRY(pl->tables.alloc(sizeof(uint32_t) * blob.size()));
+    CUDA_TRY(pl->poff.alloc(sizeof(uint64_t) * offs.size()));
+    CUDA_TRY(cudaMemcpy(pl->tables.p, blob.data(), sizeof(uint32_t) * blob.size(), cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(pl->poff.p, offs.data(), sizeof(uint64_t) * offs.size(), cudaMemcpyHostToDevice));
+    CUDA_TRY(pl->counters.alloc(2 * sizeof(unsigned long long)));
+    CUDA_TRY(pl->totals.alloc(2 * sizeof(unsigned long long) * count));
+    CUDA_TRY(pl->first_item.alloc(sizeof(unsigned long long) * count));
+    CUDA_TRY(pl->records.alloc(sizeof(emp::FirstRecord) * count));
+    CUDA_TRY(pl->flags.alloc(2 * sizeof(int)));
+    CUDA_TRY(pl->prefix_out.alloc(sizeof(uint16_t) * 256));
+    CUDA_TRY(cudaEventCreate(&pl->ev0));
+    CUDA_TRY(cudaEventCreate(&pl->ev1));
+    EMP_TRY(expand(*pl));
+    // launch geometry: as many blocks per SM as shared memory allows
+    cudaDeviceProp prop;
+    CUDA_TRY(cudaGetDeviceProperties(&prop, pl->device));
+    pl->threads = pl->cfg.threads_per_block ? pl->cfg.threads_per_block : 128;
+    if (pl->threads % 32 || pl->threads > 256)
+        return fail(EMP_ERR_INVALID, "threads_per_block must be a multiple of 32 up to 256");
+    const size_t smem = emp::dfs_smem_bytes(pl->max_levels, pl->max_avail, pl->threads);
+    if (smem > static_cast<size_t>(prop.sharedMemPerBlockOptin))
+        return fail(EMP_ERR_UNSUPPORTED, "per-thread DFS state does not fit shared memory; use fewer threads per block");
+    CUDA_TRY(cudaFuncSetAttribute(emp::dfs_kernel_symbol(), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  static_cast<int>(smem)));
+    int per_sm = 0;
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, emp::dfs_kernel_symbol(),
+                                                           static_cast<int>(pl->threads), smem));
+    if (per_sm < 1) return fail(EMP_ERR_UNSUPPORTED, "DFS kernel cannot be resident with this configuration");
+    if (pl->cfg.blocks_per_sm) per_sm = std::min<int>(per_sm, static_cast<int>(pl->cfg.blocks_per_sm));
+    pl->blocks = static_cast<uint32_t>(per_sm) * static_cast<uint32_t>(prop.multiProcessorCount);
+    CUDA_TRY(pl->spill.alloc(sizeof(uint32_t) * static_cast<size_t>(pl->blocks) * pl->threads * pl->max_levels *
+                             pl->max_kw));
+    // round queues: room for every resident thread to hand back a full path twice
+    const uint64_t resident = static_cast<uint64_t>(pl->blocks) * pl->threads;
+    pl->capacity = std::max<uint64_t>(resident * 2 * (pl->max_levels - pl->depth + 1) / 4, 1u << 16);
+    pl->capacity = std::min<uint64_t>(pl->capacity, (uint64_t)1 << 23);
+    CUDA_TRY(pl->rec_a.alloc(sizeof(uint32_t) * pl->rec_words * pl->capacity));
+    CUDA_TRY(pl->rec_b.alloc(sizeof(uint32_t) * pl->rec_words * pl->capacity));
+    pl->budget = pl->cfg.split_budget ? pl->cfg.split_budget : (1u << 15);
+    EMP_TRY(build_initial(*pl, 0, 1, pl->n_all));
+    *out = pl.release();
+    return EMP_OK;
+}
+
+extern "C" emp_status emp_bt_plan_subtrees(emp_bt_plan plan, uint64_t* subtrees)
+{
+    emp::clear_error();
+    if (!plan || !subtrees) return fail(EMP_ERR_INVALID, "emp_bt_plan_subtrees: null argument");
+    *subtrees = plan->n_all;
+    return EMP_OK;
+}
+
+extern "C" emp_status emp_bt_plan_select(emp_bt_plan plan, uint64_t first, uint64_t stride, uint64_t count)
+{
+    emp::clear_error();
+    if (!plan || !stride) return fail(EMP_ERR_INVALID, "emp_bt_plan_select: null plan or zero stride");
+    if (count && first + (count - 1) * stride >= plan->n_all)
+        return fail(EMP_ERR_INVALID, "emp_bt_plan_select: selection past the last subtree");
+    CUDA_TRY(cudaSetDevice(plan->device));
+    EMP_TRY(build_initial(*plan, first, stride, count));
+    plan->sampled = true;
+    return EMP_OK;
+}
+
+extern "C" emp_status emp_bt_plan_run(emp_bt_plan plan, void* stream)
+{
+    emp::clear_error();
+    if (!plan) return fail(EMP_ERR_INVALID, "emp_bt_plan_run: null plan");
+    CUDA_TRY(cudaSetDevice(plan->device));
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    emp::BtLaunch P = plan->launch();
+    CUDA_TRY(emp::launch_bt_reset(P, static_cast<uint32_t>(plan->puzzles.size()), st));
+    if (plan->item_nodes.p) {
+        CUDA_TRY(cudaMemsetAsync(plan->item_nodes.p, 0, plan->item_nodes.bytes, st));
+        CUDA_TRY(cudaMemsetAsync(plan->item_sols.p, 0, plan->item_sols.bytes, st));
+    }
+    CUDA_TRY(cudaEventRecord(plan->ev0, st));
+    // rounds: the initial records, then the work handed back by each round
+    const uint32_t* in = plan->rec_init.as<uint32_t>();
+    uint64_t n_in = plan->n_init;
+    DeviceBuffer* out = &plan->rec_a;
+    DeviceBuffer* spare = &plan->rec_b;
+    plan->rounds = 0;
+    while (n_in) {
+        CUDA_TRY(cudaMemsetAsync(plan->counters.p, 0, plan->counters.bytes, st));
+        P.in_rec = in;
+        P.n_in = n_in;
+        P.out_rec = out->as<uint32_t>();
+        CUDA_TRY(emp::launch_dfs(P, plan->blocks, plan->threads, st));
+        ++plan->rounds;
+        unsigned long long tail = 0;
+        CUDA_TRY(cudaMemcpyAsync(&tail, plan->counters.as<unsigned long long>() + 1, sizeof(tail),
+                                 cudaMemcpyDeviceToHost, st));
+        CUDA_TRY(cudaStreamSynchronize(st));
+        n_in = std::min<uint64_t>(tail, plan->capacity);
+        in = out->as<uint32_t>();
+        std::swap(out, spare);
+        if (plan->rounds > 100000) return fail(EMP_ERR_CUDA, "emp_bt_plan_run: too many rounds");
+    }
+    CUDA_TRY(cudaEventRecord(plan->ev1, st));
+    plan->ran = true;
+    return EMP_OK;
+}
+
+extern "C" emp_status emp_bt_plan_results(emp_bt_plan plan, emp_bt_result* results)
+{
+    emp::clear_error();
+    if (!plan || !results) return fail(EMP_ERR_INVALID, "emp_bt_plan_results: null argument");
+    if (!plan->ran) return fail(EMP_ERR_INVALID, "emp_bt_plan_results: plan has not run");
+    CUDA_TRY(cudaSetDevice(plan->device));
+    CUDA_TRY(cudaEventSynchronize(plan->ev1));
+    float ms = 0;
+    CUDA_TRY(cudaEventElapsedTime(&ms, plan->ev0, plan->ev1));
+    const uint32_t P = static_cast<uint32_t>(plan->puzzles.size());
+    std::vector<unsigned long long> tot(2 * P);
+    std::vector<emp::FirstRecord> rec(P);
+    int flags[2];
+    CUDA_TRY(cudaMemcpy(tot.data(), plan->totals.p, sizeof(unsigned long long) * 2 * P, cudaMemcpyDeviceToHost));
+    CUDA_TRY(cudaMemcpy(rec.data(), plan->records.p, sizeof(emp::FirstRecord) * P, cudaMemcpyDeviceToHost));
+    CUDA_TRY(cudaMemcpy(flags, plan->flags.p, sizeof(flags), cudaMemcpyDeviceToHost));
+    const bool aborted = (flags[1] & (emp::EMP_DEV_ABORTED | emp::EMP_DEV_TIMEOUT)) != 0;
+    for (uint32_t i = 0; i < P; ++i) {
+        emp_bt_result& r = results[i];
+        std::memset(&r, 0, sizeof(r));
+        const emp_puzzle pz = plan->puzzles[i];
+        r.subtrees = plan->n_init;
+        r.split_depth = plan->depth;
+        r.expansion_nodes = plan->exp_nodes[i];
+        r.nodes = tot[2 * i] + (plan->sampled ? 0 : plan->exp_nodes[i]);
+        r.solutions = tot[2 * i + 1] + (plan->sampled ? 0 : plan->exp_sols[i]);
+        r.status = aborted ? EMP_INCOMPLETE : EMP_OK;
+        r.kernel_ms = ms;
+        r.rounds = plan->rounds;
+        for (uint32_t pos = 0; pos < 256; ++pos) r.first_solution[pos] = 0xFFFFFFFFu;
+        if (rec[i].has && !rec[i].missed) {
+            for (uint32_t l = 0; l < pz->model.n; ++l) {
+                const emp::LevelPlan& lp = pz->plan[l];
+                const uint32_t t = rec[i].t[l];
+                const uint32_t piece = pz->model.members[lp.kind][t >> 2];
+                r.first_solution[lp.position] = (piece << 2) | (t & 3u);
+            }
+            r.has_first_solution = 1;
+        }
+    }
+    return EMP_OK;
+}
+
+extern "C" emp_status emp_bt_plan_subtree_counts(emp_bt_plan plan, uint64_t* nodes, uint64_t* solutions,
+                                                 uint64_t capacity)
+{
+    emp::clear_error();
+    if (!plan || !nodes || !solutions) return fail(EMP_ERR_INVALID, "emp_bt_plan_subtree_counts: null argument");
+    if (!plan->item_nodes.p) return fail(EMP_ERR_INVALID, "emp_bt_plan_subtree_counts: keep_subtree_counts was 0");
+    const uint64_t n = std::min<uint64_t>(capacity, plan->n_init);
+    CUDA_TRY(cudaSetDevice(plan->device));
+    CUDA_TRY(cudaDeviceSynchronize());
+    CUDA_TRY(cudaMemcpy(nodes, plan->item_nodes.p, sizeof(uint64_t) * n, cudaMemcpyDeviceToHost));
+    CUDA_TRY(cudaMemcpy(solutions, plan->item_sols.p, sizeof(uint64_t) * n, cudaMemcpyDeviceToHost));
+    return EMP_OK;
+}
+
+extern "C" emp_status emp_bt_plan_subtree_prefix(emp_bt_plan plan, uint64_t index, uint16_t* prefix, uint32_t capacity)
+{
+    emp::clear_error();
+    if (!plan || !prefix) return fail(EMP_ERR_INVALID, "emp_bt_plan_subtree_prefix: null argument");
+    if (index >= plan->n_init || capacity < plan->depth) return fail(EMP_ERR_INVALID, "emp_bt_plan_subtree_prefix: bad index");
+    CUDA_TRY(cudaSetDevice(plan->device));
+    CUDA_TRY(emp::launch_record_prefix(plan->rec_init.as<uint32_t>(), plan->rec_words, index,
+                                       plan->prefix_out.as<uint16_t>(), nullptr));
+    CUDA_TRY(cudaMemcpy(prefix, plan->prefix_out.p, sizeof(uint16_t) * plan->depth, cudaMemcpyDeviceToHost));
+    return EMP_OK;
+}
+
+extern "C" void emp_bt_plan_destroy(emp_bt_plan plan)
+{
+    if (plan) {
+        cudaSetDevice(plan->device);
+        delete plan;
+    }
+}
+
+extern "C" emp_status emp_bt_count_batch(const emp_puzzle* puzzles, uint32_t count, const emp_bt_config* config,
+                                         emp_bt_result* results)
+{
+    const auto t0 = std::chrono::steady_clock::now();
+    emp_bt_plan plan = nullptr;
+    emp_status s = emp_bt_plan_create(puzzles, count, config, &plan);
+    if (s != EMP_OK) return s;
+    std::unique_ptr<emp_bt_plan_t> guard(plan);
+    s = emp_bt_plan_run(plan, nullptr);
+    if (s != EMP_OK) return s;
+    s = emp_bt_plan_results(plan, results);
+    if (s != EMP_OK) return s;
+    guard.reset();
+    const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    bool incomplete = false;
+    for (uint32_t i = 0; i < count; ++i) {
+        results[i].total_ms = ms;
+        incomplete |= results[i].status == EMP_INCOMPLETE;
+    }
+    return incomplete ? EMP_INCOMPLETE : EMP_OK;
+}
+
+extern "C" emp_status emp_bt_count(emp_puzzle puzzle, const emp_bt_config* config, emp_bt_result* result)
+{
+    return emp_bt_count_batch(&puzzle, 1, config, result);
+}

@@ -1,0 +1,667 @@
+// Exhaustive backtracker kernels for sm_100a.
+//
+// Work decomposition (the reference runs one warp on one tree, never split,
+// src/CUDA_backtracker.cu:190-214; this build splits the tree):
+//   1. prefix expansion, level by level up to the split depth d: one thread per
+//      parent prefix walks the candidate set of its next level in the
+//      reference's order, applying identical-piece masks exactly as
+//      emp_position_strategy::select_piece does; a count pass, an exclusive
+//      scan and an emit pass keep the prefixes in the reference's DFS order;
+//   2. a persistent DFS kernel: every thread owns one subtree at a time, pops
+//      subtree ids from a global queue (one atomic per warp, distributed with
+//      ballot/shuffle) and walks it with its stack in shared memory.
+//
+// Per-thread DFS state lives in shared memory, thread-interleaved so that a
+// warp touching "its" entries hits 32 distinct banks:
+//   stk[L*T + tid]  = t << 21 | spilled << 20 | colours of the placed piece
+//   av[w*T + tid]   = availability words of all three kinds
+// The identical-piece case needs the exact remaining-candidate set of a level
+// once a transition with a non-trivial mask has been tried there; such a level
+// keeps its set in a per-thread global scratch row (spill) until it is left.
+#include "emp_bt.h"
+#include "emp_bt_kernels.cuh"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+
+namespace emp {
+
+using namespace dev;
+
+namespace {
+
+constexpr unsigned kFull = 0xFFFFFFFFu;
+constexpr uint32_t kMaxExpandDepth = 64;
+constexpr uint32_t kMaxAvailWords = 96;
+
+__device__ __forceinline__ uint64_t global_ns()
+{
+    uint64_t t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
+}
+
+// ---------------------------------------------------------------------------
+// Prefix expansion.  mode 0: count children; mode 1: write children.
+__global__ void expand_kernel(BtLaunch P, const uint16_t* __restrict__ parents,
+                              const uint32_t* __restrict__ parent_puzzle, uint64_t n_parents,
+                              uint32_t level, uint32_t* __restrict__ counts,
+                              const uint64_t* __restrict__ offsets, uint16_t* __restrict__ children,
+                              uint32_t* __restrict__ child_puzzle, unsigned long long* __restrict__ level_nodes,
+                              unsigned long long* __restrict__ level_sols, int mode)
+{
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n_parents;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t pz = parent_puzzle ? parent_puzzle[i] : 0u;
+        const uint32_t* tb = P.tables + P.puzzle_offset[pz];
+        const uint32_t n = ldg(tb + H_N), ncol = ldg(tb + H_NCOL);
+        uint32_t av[kMaxAvailWords];
+        uint32_t cols[kMaxExpandDepth];
+        const uint32_t aw = ldg(tb + H_AWORDS);
+        for (uint32_t w = 0; w < aw; ++w) av[w] = ldg(tb + ldg(tb + H_INIT) + w);
+        const uint16_t* pre = parents + i * level;
+        for (uint32_t l = 0; l < level; ++l) {
+            const LevelDesc d = load_desc(tb, l);
+            const uint32_t t = pre[l];
+            av[d.aoff + (t >> 5)] &= ~(0xFu << (t & 28u));
+            cols[l] = ldg(tb + ldg(tb + H_TINFO + d.kind) + t) & 0xFFFFFu;
+        }
+        uint32_t cnt = 0;
+        if (level < n) {
+            const LevelDesc d = load_desc(tb, level);
+            const uint32_t* sm[4];
+            for (uint32_t j = 0; j < d.nplaced; ++j) {
+                const uint32_t s = desc_side(d, j);
+                const uint32_t c = (cols[desc_nb(d, j)] >> (5 * ((s + 2) & 3))) & 31u;
+                sm[j] = tb + ldg(tb + H_SIDE + d.kind) + (s * ncol + c) * d.kw;
+            }
+            uint32_t R[32];
+            for (uint32_t w = 0; w < d.kw; ++w) {
+                uint32_t x = ldg(tb + d.base + w) & av[d.aoff + w];
+                for (uint32_t j = 0; j < d.nplaced; ++j) x &= ldg(sm[j] + w);
+                R[w] = x;
+            }
+            const uint32_t* extra = tb + ldg(tb + H_EXTRA + d.kind);
+            const uint32_t* tinfo = tb + ldg(tb + H_TINFO + d.kind);
+            uint64_t out = mode ? offsets[i] : 0;
+            for (uint32_t w = 0; w < d.kw; ++w) {
+                while (R[w]) {
+                    const uint32_t t = w * 32 + __ffs(R[w]) - 1;
+                    if (mode) {
+                        uint16_t* c = children + out * (level + 1);
+                        for (uint32_t l = 0; l < level; ++l) c[l] = pre[l];
+                        c[level] = static_cast<uint16_t>(t);
+                        if (child_puzzle) child_puzzle[out] = pz;
+                        ++out;
+                    }
+                    ++cnt;
+                    if (level == 0) { R[w] = 0; w = d.kw; break; }  // position 0 keeps its first transition
+                    if ((ldg(tinfo + t) >> 20) & 1u) {
+                        for (uint32_t ww = 0; ww < d.kw; ++ww) R[ww] &= ldg(extra + t * d.kw + ww);
+                    } else {
+                        R[w] &= ~(1u << (t & 31));
+                    }
+                }
+            }
+        }
+        if (!mode) {
+            counts[i] = cnt;
+            if (cnt) {
+                atomicAdd(&level_nodes[pz], (unsigned long long)cnt);
+                if (level == n - 1) atomicAdd(&level_sols[pz], (unsigned long long)cnt);
+            }
+        }
+    }
+}
+
+// Exclusive scan of u32 counts into u64 offsets: per-block sums, then one
+// block scans the block sums, then each block scans its slice.
+constexpr uint32_t kScanBlock = 1024;
+
+__device__ uint64_t block_exclusive_scan(uint64_t v, uint64_t* sh, uint64_t& total)
+{
+    const uint32_t tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    uint64_t x = v;
+    for (int o = 1; o < 32; o <<= 1) {
+        uint64_t y = __shfl_up_sync(kFull, x, o);
+        if (lane >= (uint32_t)o) x += y;
+    }
+    if (lane == 31) sh[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+        uint64_t s = lane < (blockDim.x >> 5) ? sh[lane] : 0;
+        for (int o = 1; o < 32; o <<= 1) {
+            uint64_t y = __shfl_up_sync(kFull, s, o);
+            if (lane >= (uint32_t)o) s += y;
+        }
+        sh[lane] = s;
+    }
+    __syncthreads();
+    const uint64_t before = wid ? sh[wid - 1] : 0;
+    total = sh[(blockDim.x >> 5) - 1];
+    __syncthreads();
+    return before + x - v;
+}
+
+__global__ void scan_block_sums(const uint32_t* __restrict__ in, uint64_t n, uint64_t* __restrict__ sums)
+{
+    __shared__ uint64_t sh[32];
+    const uint64_t i = blockIdx.x * (uint64_t)kScanBlock + threadIdx.x;
+    uint64_t total;
+    block_exclusive_scan(i < n ? in[i] : 0, sh, total);
+    if (threadIdx.x == 0) sums[blockIdx.x] = total;
+}
+
+__global__ void scan_sums_serial(uint64_t* __restrict__ sums, uint64_t nblocks, uint64_t* __restrict__ grand)
+{
+    __shared__ uint64_t sh[32];
+    uint64_t carry = 0;
+    for (uint64_t b0 = 0; b0 < nblocks; b0 += kScanBlock) {
+        const uint64_t i = b0 + threadIdx.x;
+        const uint64_t v = i < nblocks ? sums[i] : 0;
+        uint64_t total;
+        const uint64_t ex = block_exclusive_scan(v, sh, total);
+        if (i < nblocks) sums[i] = carry + ex;
+        carry += total;
+    }
+    if (threadIdx.x == 0) *grand = carry;
+}
+
+__global__ void scan_apply(const uint32_t* __restrict__ in, uint64_t n, const uint64_t* __restrict__ sums,
+                           uint64_t* __restrict__ out)
+{
+    __shared__ uint64_t sh[32];
+    const uint64_t i = blockIdx.x * (uint64_t)kScanBlock + threadIdx.x;
+    uint64_t total;
+    const uint64_t ex = block_exclusive_scan(i < n ? in[i] : 0, sh, total);
+    if (i < n) out[i] = sums[blockIdx.x] + ex;
+}
+
+
+// ---------------------------------------------------------------------------
+// Persistent subtree DFS over work records.
+//
+// A work record is "prefix t[0..len-1], resume bit `start` at level len"
+// (plus the exact remaining set of level len when it is spilled).  The initial
+// records are the split-depth prefixes with start 0.  A thread that spends
+// more than `item_budget` steps on a record hands its remaining work back as
+// one record per level that still has candidates (the current level from its
+// resume bit, every shallower level from its next sibling) for the next round,
+// so a huge subtree spreads over the GPU in a few rounds.
+//
+// record words: [0,1] subtree id (for per-subtree counts), [2] len | start<<16,
+// [3] puzzle | spilled<<16 | empty<<17, [4..] transitions (u16 pairs), then
+// the remaining set of level len (max_kw words).
+struct ThreadItem {
+    uint64_t orig;
+    const uint32_t* tb;
+    uint32_t pz, n, ncol, L, base, start, spilled;
+    uint64_t nodes, sols, steps;
+    bool active;
+};
+
+__device__ __forceinline__ uint32_t rec_t(const uint32_t* rec, uint32_t l)
+{
+    return (rec[4 + (l >> 1)] >> (16 * (l & 1))) & 0xFFFFu;
+}
+
+__device__ __forceinline__ void load_record(const BtLaunch& P, ThreadItem& s, const uint32_t* rec, uint32_t* stk,
+                                            uint32_t* av, uint32_t* spill, uint32_t T, uint32_t tid)
+{
+    s.orig = static_cast<uint64_t>(rec[0]) | (static_cast<uint64_t>(rec[1]) << 32);
+    const uint32_t len = rec[2] & 0xFFFFu;
+    s.start = rec[2] >> 16;
+    s.pz = rec[3] & 0xFFFFu;
+    s.spilled = (rec[3] >> 16) & 1u;
+    s.tb = P.tables + P.puzzle_offset[s.pz];
+    s.n = ldg(s.tb + H_N);
+    s.ncol = ldg(s.tb + H_NCOL);
+    const uint32_t aw = ldg(s.tb + H_AWORDS);
+    const uint32_t init = ldg(s.tb + H_INIT);
+    for (uint32_t w = 0; w < aw; ++w) av[w * T + tid] = ldg(s.tb + init + w);
+    for (uint32_t l = 0; l < len; ++l) {
+        const LevelDesc d = load_desc(s.tb, l);
+        const uint32_t t = rec_t(rec, l);
+        av[(d.aoff + (t >> 5)) * T + tid] &= ~(0xFu << (t & 28u));
+        stk[l * T + tid] = (t << 21) | (ldg(s.tb + ldg(s.tb + H_TINFO + d.kind) + t) & 0xFFFFFu);
+    }
+    if (s.spilled) {
+        const uint32_t* R = rec + P.rec_r_off;
+        for (uint32_t w = 0; w < P.max_kw; ++w) spill[len * P.max_kw + w] = R[w];
+    }
+    s.L = len;
+    s.base = len;
+    s.nodes = 0;
+    s.sols = 0;
+    s.steps = 0;
+    s.active = true;
+}
+
+// Candidates of the current level from bit `start` on, first non-empty word.
+struct Scan {
+    uint32_t w, x;
+};
+
+__device__ __forceinline__ Scan scan_level(const BtLaunch& P, const ThreadItem& s, const LevelDesc& d,
+                                           const uint32_t* const* sm, const uint32_t* stk, const uint32_t* av,
+                                           const uint32_t* sp, uint32_t start, bool spilled, uint32_t T,
+                                           uint32_t tid)
+{
+    Scan r{start >> 5, 0};
+    for (; r.w < d.kw; ++r.w) {
+        uint32_t x;
+        if (spilled) {
+            x = sp[r.w];
+        } else {
+            x = ldg(s.tb + d.base + r.w) & av[(d.aoff + r.w) * T + tid];
+            for (uint32_t j = 0; j < d.nplaced; ++j) x &= ldg(sm[j] + r.w);
+        }
+        if (r.w == (start >> 5)) x &= ~0u << (start & 31u);
+        if (x) {
+            r.x = x;
+            break;
+        }
+    }
+    return r;
+}
+
+__device__ __forceinline__ void side_masks(const ThreadItem& s, const LevelDesc& d, const uint32_t* stk, uint32_t T,
+                                           uint32_t tid, const uint32_t** sm)
+{
+    for (uint32_t j = 0; j < d.nplaced; ++j) {
+        const uint32_t sd = desc_side(d, j);
+        const uint32_t c = (stk[desc_nb(d, j) * T + tid] >> (5 * ((sd + 2) & 3))) & 31u;
+        sm[j] = s.tb + ldg(s.tb + H_SIDE + d.kind) + (sd * s.ncol + c) * d.kw;
+    }
+}
+
+// One step of emp_strategy::specific_run (include/emp_strategy.h:352-401)
+// inside the thread's record.  Returns false once the record is exhausted.
+__device__ __forceinline__ bool dfs_step(const BtLaunch& P, ThreadItem& s, uint32_t* stk, uint32_t* av,
+                                         uint32_t* spill, uint32_t T, uint32_t tid, bool* solved)
+{
+    const LevelDesc d = load_desc(s.tb, s.L);
+    const uint32_t* sm[4];
+    side_masks(s, d, stk, T, tid, sm);
+    uint32_t* sp = spill + s.L * P.max_kw;
+    const Scan c = scan_level(P, s, d, sm, stk, av, sp, s.start, s.spilled, T, tid);
+    if (c.w < d.kw) {
+        const uint32_t t = c.w * 32 + __ffs(c.x) - 1;
+        const uint32_t ti = ldg(s.tb + ldg(s.tb + H_TINFO + d.kind) + t);
+        if ((ti >> 20) & 1u) {
+            // select_piece with an identical mask that clears other candidates
+            // (emp_position_strategy.h:197-200): the level keeps its exact
+            // remaining set from now on
+            const uint32_t* ex = s.tb + ldg(s.tb + H_EXTRA + d.kind) + t * d.kw;
+            for (uint32_t ww = 0; ww < d.kw; ++ww) {
+                uint32_t r;
+                if (s.spilled) {
+                    r = sp[ww];
+                } else {
+                    r = ldg(s.tb + d.base + ww) & av[(d.aoff + ww) * T + tid];
+                    for (uint32_t j = 0; j < d.nplaced; ++j) r &= ldg(sm[j] + ww);
+                }
+                sp[ww] = r & ldg(ex + ww);
+            }
+            s.spilled = 1;
+        }
+        av[(d.aoff + (t >> 5)) * T + tid] &= ~(0xFu << (t & 28u));
+        stk[s.L * T + tid] = (t << 21) | (s.spilled << 20) | (ti & 0xFFFFFu);
+        ++s.nodes;
+        if (s.L == s.n - 1) {
+            // solution: count it, give the piece back, try the next candidate
+            ++s.sols;
+            *solved = true;
+            av[(d.aoff + (t >> 5)) * T + tid] |= 0xFu << (t & 28u);
+            s.start = t + 1;
+        } else {
+            ++s.L;
+            s.start = 0;
+            s.spilled = 0;
+        }
+        return true;
+    }
+    if (s.L == s.base) return false;
+    --s.L;
+    const uint32_t e = stk[s.L * T + tid];
+    const uint32_t t = e >> 21;
+    s.spilled = (e >> 20) & 1u;
+    const LevelDesc dl = load_desc(s.tb, s.L);
+    av[(dl.aoff + (t >> 5)) * T + tid] |= 0xFu << (t & 28u);
+    s.start = t + 1;
+    return true;
+}
+
+// Keeps the lexicographically smallest solution path of each puzzle: in the
+// reference's visiting order (ascending candidate bit at every level) that is
+// its first solution.  The lock is held for a few hundred cycles; the wait for
+// it is bounded and a thread that gives up flags the record as unreliable.
+__device__ void record_solution(const BtLaunch& P, const ThreadItem& s, const uint32_t* stk, uint32_t T,
+                                uint32_t tid)
+{
+    FirstRecord* r = P.first_records + s.pz;
+    atomicMin(&P.first_item[s.pz], (unsigned long long)s.orig);
+    if (s.orig > *(volatile unsigned long long*)&P.first_item[s.pz]) return;
+    bool locked = false;
+    for (int tries = 0; tries < 4096; ++tries) {
+        if (atomicCAS(&r->lock, 0u, 1u) == 0u) {
+            locked = true;
+            break;
+        }
+        __nanosleep(64);
+    }
+    if (!locked) {
+        atomicExch(&r->missed, 1u);
+        return;
+    }
+    __threadfence();
+    bool better = !r->has;
+    if (!better) {
+        for (uint32_t l = 0; l < s.n; ++l) {
+            const uint32_t mine = stk[l * T + tid] >> 21, theirs = r->t[l];
+            if (mine != theirs) {
+                better = mine < theirs;
+                break;
+            }
+        }
+    }
+    if (better) {
+        for (uint32_t l = 0; l < s.n; ++l) r->t[l] = static_cast<uint16_t>(stk[l * T + tid] >> 21);
+        r->has = 1;
+    }
+    __threadfence();
+    atomicExch(&r->lock, 0u);
+}
+
+__device__ __forceinline__ void account(const BtLaunch& P, const ThreadItem& s)
+{
+    if (s.nodes) atomicAdd(&P.totals[2 * s.pz], (unsigned long long)s.nodes);
+    if (s.sols) atomicAdd(&P.totals[2 * s.pz + 1], (unsigned long long)s.sols);
+    if (P.item_nodes) {
+        if (s.nodes) atomicAdd(&P.item_nodes[s.orig], (unsigned long long)s.nodes);
+        if (s.sols) atomicAdd(&P.item_sols[s.orig], (unsigned long long)s.sols);
+    }
+}
+
+// Remaining candidates of level l (current level: from s.start; shallower
+// levels: after their placed transition), with `av` holding the availability
+// of level l's entry.
+__device__ __forceinline__ bool level_has_work(const BtLaunch& P, const ThreadItem& s, uint32_t l, const uint32_t* stk,
+                                               const uint32_t* av, const uint32_t* spill, uint32_t T, uint32_t tid,
+                                               uint32_t* start_out, uint32_t* spilled_out)
+{
+    const LevelDesc d = load_desc(s.tb, l);
+    uint32_t start, spilled;
+    if (l == s.L) {
+        start = s.start;
+        spilled = s.spilled;
+    } else {
+        const uint32_t e = stk[l * T + tid];
+        start = (e >> 21) + 1;
+        spilled = (e >> 20) & 1u;
+    }
+    const uint32_t* sm[4];
+    side_masks(s, d, stk, T, tid, sm);
+    const Scan c = scan_level(P, s, d, sm, stk, av, spill + l * P.max_kw, start, spilled != 0, T, tid);
+    *start_out = start;
+    *spilled_out = spilled;
+    return c.w < d.kw;
+}
+
+__device__ __forceinline__ void toggle_piece(const ThreadItem& s, uint32_t l, const uint32_t* stk, uint32_t* av,
+                                             uint32_t T, uint32_t tid, bool give_back)
+{
+    const LevelDesc d = load_desc(s.tb, l);
+    const uint32_t t = stk[l * T + tid] >> 21;
+    if (give_back) av[(d.aoff + (t >> 5)) * T + tid] |= 0xFu << (t & 28u);
+    else av[(d.aoff + (t >> 5)) * T + tid] &= ~(0xFu << (t & 28u));
+}
+
+// Hands the remaining work of the thread's record to the next round: one
+// record per level that still holds candidates.  Pass 1 walks the levels from
+// the current one up, giving each level's piece back to get that level's entry
+// availability, and counts; pass 2 walks back down, writing records and taking
+// the pieces again, which leaves the state as it was.  Returns false when the
+// output queue is full (the thread then keeps the work).
+__device__ bool split_record(const BtLaunch& P, ThreadItem& s, uint32_t* stk, uint32_t* av, const uint32_t* spill,
+                             uint32_t T, uint32_t tid)
+{
+    uint32_t cnt = 0, start, spilled;
+    for (uint32_t l = s.L + 1; l-- > s.base;) {
+        if (l < s.L) toggle_piece(s, l, stk, av, T, tid, true);
+        cnt += level_has_work(P, s, l, stk, av, spill, T, tid, &start, &spilled);
+    }
+    const unsigned long long slot = cnt ? atomicAdd(P.out_tail, (unsigned long long)cnt) : 0ull;
+    const bool fits = slot + cnt <= P.out_capacity;
+    unsigned long long k = slot;
+    for (uint32_t l = s.base; l <= s.L; ++l) {
+        if (level_has_work(P, s, l, stk, av, spill, T, tid, &start, &spilled)) {
+            if (fits) {
+                uint32_t* rec = P.out_rec + k * P.rec_words;
+                rec[0] = static_cast<uint32_t>(s.orig);
+                rec[1] = static_cast<uint32_t>(s.orig >> 32);
+                rec[2] = l | (start << 16);
+                rec[3] = s.pz | (spilled << 16);
+                for (uint32_t j = 0; j < l; j += 2) {
+                    const uint32_t lo = stk[j * T + tid] >> 21;
+                    const uint32_t hi = j + 1 < l ? stk[(j + 1) * T + tid] >> 21 : 0u;
+                    rec[4 + (j >> 1)] = lo | (hi << 16);
+                }
+                if (spilled)
+                    for (uint32_t w = 0; w < P.max_kw; ++w) rec[P.rec_r_off + w] = spill[l * P.max_kw + w];
+            } else if (k < P.out_capacity) {
+                P.out_rec[k * P.rec_words + 3] = 1u << 17;  // reserved slot that fits: mark empty
+            }
+            ++k;
+        }
+        if (l < s.L) toggle_piece(s, l, stk, av, T, tid, false);
+    }
+    return fits;
+}
+
+template <int kStepsPerFetch>
+__global__ void __launch_bounds__(256) dfs_kernel(BtLaunch P)
+{
+    extern __shared__ uint32_t smem[];
+    const uint32_t T = blockDim.x, tid = threadIdx.x, lane = tid & 31;
+    uint32_t* stk = smem;
+    uint32_t* av = smem + P.max_levels * T;
+    uint32_t* spill = P.spill + (size_t)(blockIdx.x * T + tid) * P.max_levels * P.max_kw;
+    ThreadItem s;
+    s.active = false;
+    bool alive = true;
+    uint32_t since_check = 0;  // steps since the last look at the global flags
+    const uint64_t deadline = P.timeout_ns ? global_ns() + P.timeout_ns : 0;
+    const uint32_t lt_mask = (1u << lane) - 1u;
+
+    for (;;) {
+        // ---- work fetch: one atomic per warp, ranks from the ballot ----
+        const bool need = alive && !s.active;
+        const unsigned needmask = __ballot_sync(kFull, need);
+        if (needmask) {
+            const uint32_t leader = __ffs(needmask) - 1;
+            unsigned long long base = 0;
+            if (lane == leader) base = atomicAdd(P.cursor, (unsigned long long)__popc(needmask));
+            base = __shfl_sync(kFull, base, leader);
+            if (need) {
+                const uint64_t my = base + __popc(needmask & lt_mask);
+                if (my < P.n_in && !*(volatile int*)P.abort_flag) {
+                    const uint32_t* rec = P.in_rec + my * P.rec_words;
+                    if (!((rec[3] >> 17) & 1u)) {
+                        load_record(P, s, rec, stk, av, spill, T, tid);
+                        if (P.stop_at_first && s.orig > *(volatile unsigned long long*)&P.first_item[s.pz])
+                            s.active = false;  // a lower subtree of this puzzle holds a solution
+                    }
+                } else {
+                    alive = false;
+                }
+            }
+        }
+        if (!__any_sync(kFull, alive)) break;
+
+        // ---- DFS steps ----
+        for (int step = 0; step < kStepsPerFetch && s.active; ++step) {
+            bool solved = false;
+            if (dfs_step(P, s, stk, av, spill, T, tid, &solved)) {
+                if (solved) record_solution(P, s, stk, T, tid);
+                continue;
+            }
+            account(P, s);
+            s.active = false;
+        }
+        if (!s.active) continue;
+        s.steps += kStepsPerFetch;
+        since_check += kStepsPerFetch;
+
+        // ---- hand work back once over budget ----
+        if (P.item_budget && s.steps >= P.item_budget) {
+            if (split_record(P, s, stk, av, spill, T, tid)) {
+                account(P, s);
+                s.active = false;
+                continue;
+            }
+            s.steps = 0;
+        }
+        // ---- deadline, cancellation and stop-at-first, every 4096 steps ----
+        if (since_check >= 4096) {
+            since_check = 0;
+            bool stop = *(volatile int*)P.abort_flag != 0;
+            if (deadline && global_ns() > deadline) {
+                stop = true;
+                atomicOr(P.status, EMP_DEV_TIMEOUT);
+            }
+            const bool superseded =
+                P.stop_at_first && s.orig > *(volatile unsigned long long*)&P.first_item[s.pz];
+            if (superseded || stop) {
+                account(P, s);
+                s.active = false;
+                if (stop) {
+                    atomicExch(P.abort_flag, 1);
+                    atomicOr(P.status, EMP_DEV_ABORTED);
+                    alive = false;
+                } else {
+                    atomicOr(P.status, EMP_DEV_SUPERSEDED);
+                }
+            }
+        }
+    }
+}
+
+__global__ void reset_kernel(BtLaunch P, uint32_t n_puzzles)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) {
+        P.abort_flag[0] = 0;
+        P.status[0] = 0;
+    }
+    if (i < n_puzzles) {
+        P.totals[2 * i] = 0;
+        P.totals[2 * i + 1] = 0;
+        P.first_item[i] = ~0ull;
+        P.first_records[i].lock = 0;
+        P.first_records[i].missed = 0;
+        P.first_records[i].has = 0;
+    }
+}
+
+// Initial records from split-depth prefixes (a strided selection of them).
+__global__ void make_records(const uint16_t* __restrict__ prefixes, const uint32_t* __restrict__ prefix_puzzle,
+                             uint32_t depth, uint64_t first, uint64_t stride, uint64_t count, uint32_t rec_words,
+                             uint32_t* __restrict__ rec)
+{
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < count;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t j = first + i * stride;
+        uint32_t* r = rec + i * rec_words;
+        r[0] = static_cast<uint32_t>(i);
+        r[1] = static_cast<uint32_t>(i >> 32);
+        r[2] = depth;
+        r[3] = prefix_puzzle[j];
+        const uint16_t* p = prefixes + j * depth;
+        for (uint32_t l = 0; l < depth; l += 2) r[4 + (l >> 1)] = p[l] | (l + 1 < depth ? (uint32_t)p[l + 1] << 16 : 0u);
+    }
+}
+
+// Prefix (transitions) of selected subtree `i`, for the host.
+__global__ void record_prefix(const uint32_t* __restrict__ rec, uint32_t rec_words, uint64_t i, uint16_t* out)
+{
+    const uint32_t* r = rec + i * rec_words;
+    const uint32_t len = r[2] & 0xFFFFu;
+    for (uint32_t l = threadIdx.x; l < len; l += blockDim.x) out[l] = static_cast<uint16_t>(rec_t(r, l));
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// host launchers
+
+cudaError_t launch_expand(const BtLaunch& P, const uint16_t* parents, const uint32_t* parent_puzzle,
+                          uint64_t n_parents, uint32_t level, uint32_t* counts, const uint64_t* offsets,
+                          uint16_t* children, uint32_t* child_puzzle, unsigned long long* level_nodes,
+                          unsigned long long* level_sols, int mode, cudaStream_t stream)
+{
+    if (!n_parents) return cudaSuccess;
+    const uint32_t threads = 128;
+    const uint64_t blocks = std::min<uint64_t>((n_parents + threads - 1) / threads, 148ull * 64);
+    expand_kernel<<<(unsigned)blocks, threads, 0, stream>>>(P, parents, parent_puzzle, n_parents, level, counts,
+                                                            offsets, children, child_puzzle, level_nodes,
+                                                            level_sols, mode);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_scan(const uint32_t* counts, uint64_t n, uint64_t* offsets, uint64_t* block_sums,
+                        uint64_t* grand_total, cudaStream_t stream)
+{
+    if (!n) return cudaMemsetAsync(grand_total, 0, sizeof(uint64_t), stream);
+    const uint64_t nb = (n + kScanBlock - 1) / kScanBlock;
+    scan_block_sums<<<(unsigned)nb, kScanBlock, 0, stream>>>(counts, n, block_sums);
+    scan_sums_serial<<<1, kScanBlock, 0, stream>>>(block_sums, nb, grand_total);
+    scan_apply<<<(unsigned)nb, kScanBlock, 0, stream>>>(counts, n, block_sums, offsets);
+    return cudaGetLastError();
+}
+
+uint64_t scan_block_sum_words(uint64_t n) { return (n + kScanBlock - 1) / kScanBlock + 1; }
+
+size_t dfs_smem_bytes(uint32_t max_levels, uint32_t max_avail_words, uint32_t threads)
+{
+    return static_cast<size_t>(max_levels + max_avail_words) * threads * sizeof(uint32_t);
+}
+
+uint32_t record_words(uint32_t max_levels, uint32_t max_kw) { return 4 + (max_levels + 1) / 2 + max_kw; }
+
+cudaError_t launch_dfs(const BtLaunch& P, uint32_t blocks, uint32_t threads, cudaStream_t stream)
+{
+    const size_t smem = dfs_smem_bytes(P.max_levels, P.max_avail_words, threads);
+    dfs_kernel<32><<<blocks, threads, smem, stream>>>(P);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_bt_reset(const BtLaunch& P, uint32_t n_puzzles, cudaStream_t stream)
+{
+    reset_kernel<<<(n_puzzles + 255) / 256, 256, 0, stream>>>(P, n_puzzles);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_make_records(const uint16_t* prefixes, const uint32_t* prefix_puzzle, uint32_t depth,
+                                uint64_t first, uint64_t stride, uint64_t count, uint32_t rec_words, uint32_t* rec,
+                                cudaStream_t stream)
+{
+    if (!count) return cudaSuccess;
+    const uint64_t blocks = std::min<uint64_t>((count + 255) / 256, 148ull * 32);
+    make_records<<<(unsigned)blocks, 256, 0, stream>>>(prefixes, prefix_puzzle, depth, first, stride, count,
+                                                       rec_words, rec);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_record_prefix(const uint32_t* rec, uint32_t rec_words, uint64_t i, uint16_t* out,
+                                 cudaStream_t stream)
+{
+    record_prefix<<<1, 64, 0, stream>>>(rec, rec_words, i, out);
+    return cudaGetLastError();
+}
+
+const void* dfs_kernel_symbol() { return reinterpret_cast<const void*>(&dfs_kernel<32>); }
+
+}  // namespace emp

@@ -1,0 +1,74 @@
+// Launch interface of the exhaustive backtracker kernels (emp_bt.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace emp {
+
+// device status bits (BtLaunch::status)
+enum : int {
+    EMP_DEV_TIMEOUT = 1,    // the kernel passed its deadline and stopped
+    EMP_DEV_ABORTED = 2,    // stopped early (deadline or cancel flag)
+    EMP_DEV_SUPERSEDED = 8, // stop-at-first: subtrees after the first solution were cut
+};
+
+// Lexicographically smallest solution path of a puzzle (its first solution in
+// the reference's visiting order).
+struct FirstRecord {
+    unsigned int lock;
+    unsigned int missed;    // a writer gave up waiting for the lock
+    unsigned int has;
+    unsigned int pad;
+    uint16_t t[256];        // transition per level
+};
+
+struct BtLaunch {
+    const uint32_t* tables = nullptr;         // all puzzle blobs
+    const uint64_t* puzzle_offset = nullptr;  // word offset of each puzzle blob
+    uint32_t depth = 0;                       // split depth (prefix expansion)
+    uint32_t max_levels = 0;                  // max pieces over the puzzles of the launch
+    uint32_t max_avail_words = 0;             // max availability words (three kinds)
+    uint32_t max_kw = 0;                      // max words of one kind
+    uint32_t* spill = nullptr;                // [threads][max_levels][max_kw] remaining sets
+    // work records of this round and of the next one
+    const uint32_t* in_rec = nullptr;
+    uint64_t n_in = 0;
+    uint32_t* out_rec = nullptr;
+    unsigned long long* out_tail = nullptr;
+    uint64_t out_capacity = 0;
+    uint32_t rec_words = 0;                   // words per record
+    uint32_t rec_r_off = 0;                   // offset of the remaining set in a record
+    uint64_t item_budget = 0;                 // steps on a record before handing work back; 0 = never
+    unsigned long long* cursor = nullptr;     // input queue head
+    unsigned long long* totals = nullptr;     // per puzzle: [2p] nodes, [2p+1] solutions (subtrees only)
+    unsigned long long* item_nodes = nullptr; // per initial subtree (optional)
+    unsigned long long* item_sols = nullptr;
+    unsigned long long* first_item = nullptr; // per puzzle: lowest initial subtree holding a solution
+    FirstRecord* first_records = nullptr;     // per puzzle
+    unsigned long long timeout_ns = 0;        // per-launch time limit (%globaltimer), 0: none
+    int* abort_flag = nullptr;                // set by the host or by a stopping thread
+    int* status = nullptr;
+    int stop_at_first = 0;
+};
+
+cudaError_t launch_expand(const BtLaunch& P, const uint16_t* parents, const uint32_t* parent_puzzle,
+                          uint64_t n_parents, uint32_t level, uint32_t* counts, const uint64_t* offsets,
+                          uint16_t* children, uint32_t* child_puzzle, unsigned long long* level_nodes,
+                          unsigned long long* level_sols, int mode, cudaStream_t stream);
+cudaError_t launch_scan(const uint32_t* counts, uint64_t n, uint64_t* offsets, uint64_t* block_sums,
+                        uint64_t* grand_total, cudaStream_t stream);
+uint64_t scan_block_sum_words(uint64_t n);
+size_t dfs_smem_bytes(uint32_t max_levels, uint32_t max_avail_words, uint32_t threads);
+uint32_t record_words(uint32_t max_levels, uint32_t max_kw);
+cudaError_t launch_dfs(const BtLaunch& P, uint32_t blocks, uint32_t threads, cudaStream_t stream);
+cudaError_t launch_bt_reset(const BtLaunch& P, uint32_t n_puzzles, cudaStream_t stream);
+cudaError_t launch_make_records(const uint16_t* prefixes, const uint32_t* prefix_puzzle, uint32_t depth,
+                                uint64_t first, uint64_t stride, uint64_t count, uint32_t rec_words, uint32_t* rec,
+                                cudaStream_t stream);
+cudaError_t launch_record_prefix(const uint32_t* rec, uint32_t rec_words, uint64_t i, uint16_t* out,
+                                 cudaStream_t stream);
+const void* dfs_kernel_symbol();
+
+}  // namespace emp

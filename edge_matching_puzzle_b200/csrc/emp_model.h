@@ -1,0 +1,110 @@
+// Host-side puzzle model of edge_matching_puzzle_b200.
+//
+// It rebuilds, from a w x h piece list, what the reference derives in its piece
+// database (include/emp_piece_db.h) and in emp_strategy's neighbour wiring
+// (include/emp_strategy.h:159-265), and lays it out for the GPU:
+//
+//  * kinds (0 centre, 1 border, 2 corner = number of frame sides,
+//    include/emp_piece.h:122-131), kind indices in file order, auto-similarity
+//    (include/emp_piece.h:144-157) and the allowed orientation subset
+//    {o : o % 2^similarity == 0} used by the constraint table
+//    (include/emp_piece_db.h:1267-1273);
+//  * the identical-piece relation and masks with the reference's exact
+//    comparison rules (include/emp_piece.h:193-220, emp_piece_db.h:528-540,
+//    830-884);
+//  * per-side colour masks replacing the reference's 2^(4*cs) constraint table:
+//    table[code] == AND over constrained sides s of side_mask[kind][s][colour]
+//    (a code constrains exactly the sides whose slot is non-zero and the
+//    table's kind is the count of frame slots, emp_piece_db.h:1281-1309), so the
+//    candidate set of a level is base[level] & side masks of its placed
+//    neighbours & availability;
+//  * a level plan for a position order (row-major "basic" or spiral).
+//
+// Candidate bit t = (kind_index << 2) | orientation, stored in 32-bit words:
+// word t >> 5, bit t & 31, i.e. one nibble per piece (8 pieces per word).
+#pragma once
+
+#include <array>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace emp {
+
+constexpr uint32_t kMaxPieces = 256;
+constexpr uint32_t kMaxColourId = 31;   // colours are packed on 5 bits on the GPU
+constexpr uint32_t kMaxLevels = 256;
+
+enum Kind : uint32_t { kCenter = 0, kBorder = 1, kCorner = 2 };
+
+struct PuzzleModel {
+    uint32_t width = 0, height = 0, n = 0;
+    std::vector<std::array<uint8_t, 4>> colours;  // per piece index: N,E,S,W
+    std::vector<uint8_t> kind, similarity;
+    std::vector<uint32_t> kind_index;
+    std::array<std::vector<uint32_t>, 3> members;   // piece index per (kind, kind index)
+    uint32_t max_colour = 0, border_id = 0;         // border_id = max colour + 1
+    std::array<uint32_t, 3> kind_words{};           // 32-bit words per kind bitfield
+    bool has_identical = false;
+    bool identical_out_of_range = false;
+    // identical masks per kind: [4*nk][kind_words] (all ones except cleared bits)
+    std::array<std::vector<uint32_t>, 3> idmask;
+
+    uint32_t nb_kind(uint32_t k) const { return static_cast<uint32_t>(members[k].size()); }
+    // colour of side s (0..3) of piece index p in orientation o (emp_piece.h:173-178)
+    uint32_t colour(uint32_t p, uint32_t s, uint32_t o) const { return colours[p][(s + o) & 3]; }
+    bool allowed(uint32_t p, uint32_t o) const { return (o % (1u << similarity[p])) == 0; }
+};
+
+// Builds the model; returns false with a message on malformed input.
+bool build_model(uint32_t width, uint32_t height, const uint8_t* colours, PuzzleModel& m,
+                 std::string& error);
+
+// Positions in visiting order: y*w+x.
+std::vector<uint32_t> order_basic(uint32_t w, uint32_t h);
+std::vector<uint32_t> order_spiral(uint32_t w, uint32_t h);
+
+// Per level of a position order.
+struct LevelPlan {
+    uint32_t position = 0;
+    uint32_t kind = 0;
+    uint32_t nplaced = 0;              // neighbours placed at lower levels
+    std::array<uint8_t, 4> side{};     // my side facing the placed neighbour
+    std::array<uint8_t, 4> nb_level{}; // level of that neighbour
+    std::vector<uint32_t> base;        // frame-side masks & allowed orientations
+};
+
+// Flattened tables consumed by the GPU kernels (one blob per puzzle).
+// Offsets are in 32-bit words from the start of the blob.
+struct DeviceTables {
+    std::vector<uint32_t> blob;
+    uint32_t n = 0, ncol = 0;           // ncol = border_id + 1
+    std::array<uint32_t, 3> kw{};       // words per kind
+    std::array<uint32_t, 3> avail_off{};// offset of each kind in the per-thread availability
+    uint32_t avail_words = 0;
+    uint32_t side_off = 0;   // [k][s][c][kw[k]] with kind base offsets side_kind_off
+    std::array<uint32_t, 3> side_kind_off{};
+    uint32_t base_off = 0;   // per level: base_level_off[L]
+    uint32_t desc_off = 0;   // per level: 2 words
+    uint32_t tinfo_off = 0;  // [k][4nk]: colours (5 bits x 4) | has_extra << 20
+    std::array<uint32_t, 3> tinfo_kind_off{};
+    uint32_t extra_off = 0;  // [k][4nk][kw] extra identical clears (all ones = none)
+    std::array<uint32_t, 3> extra_kind_off{};
+    uint32_t init_avail_off = 0;
+    uint32_t tcount_off = 0; // transitions per kind
+};
+
+bool build_plan(const PuzzleModel& m, const std::vector<uint32_t>& order,
+                std::vector<LevelPlan>& plan, std::string& error);
+
+// Lays the tables out; the header of the blob (first kHeaderWords words) holds
+// the offsets so a kernel can read everything from one pointer.
+constexpr uint32_t kHeaderWords = 32;
+void build_device_tables(const PuzzleModel& m, const std::vector<LevelPlan>& plan,
+                         DeviceTables& t);
+
+// Seeded generator (splitmix64 stream; see edge_matching_puzzle_b200/puzzle.py).
+void generate_puzzle(uint32_t w, uint32_t h, uint32_t border_colours, uint32_t interior_colours,
+                     uint64_t seed, uint8_t* out_colours);
+
+}  // namespace emp

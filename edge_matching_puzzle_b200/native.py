@@ -1,0 +1,236 @@
+"""ctypes binding of the C ABI in include/emp_b200.h (libemp_b200.so).
+
+There is no Python or CPU implementation of the search behind these calls: if the
+native library is missing or cannot load, ``load()`` raises.  The calls mirror the
+reference's launchers (launch_CUDA_backtracker, launch_CUDA_glutton_max) with results
+returned instead of printed.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import List, Optional, Sequence
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libemp_b200.so")
+
+EMP_OK = 0
+EMP_INCOMPLETE = 1
+EMP_ERR_INVALID = -1
+EMP_ERR_UNSUPPORTED = -2
+EMP_ERR_CUDA = -3
+EMP_ERR_NOMEM = -4
+
+u8p = ctypes.POINTER(ctypes.c_uint8)
+u16p = ctypes.POINTER(ctypes.c_uint16)
+u64p = ctypes.POINTER(ctypes.c_uint64)
+
+
+class EmpError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"emp status {status}: {message}")
+        self.status = status
+
+
+class PuzzleDesc(ctypes.Structure):
+    _fields_ = [("width", ctypes.c_uint32), ("height", ctypes.c_uint32), ("colours", u8p), ("order", u16p)]
+
+
+class PuzzleInfo(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_uint32) for n in ("width", "height", "nb_pieces", "nb_center", "nb_border", "nb_corner",
+                                               "border_color_id", "has_identical", "identical_masks_with_extra")]
+
+
+class BtConfig(ctypes.Structure):
+    _fields_ = [
+        ("split_depth", ctypes.c_uint32),
+        ("threads_per_block", ctypes.c_uint32),
+        ("blocks_per_sm", ctypes.c_uint32),
+        ("stop_at_first", ctypes.c_uint32),
+        ("reserved_budget", ctypes.c_uint64),
+        ("timeout_ms", ctypes.c_uint32),
+        ("device", ctypes.c_int32),
+        ("keep_subtree_counts", ctypes.c_uint32),
+        ("split_budget", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32 * 6),
+    ]
+
+
+class BtResult(ctypes.Structure):
+    _fields_ = [
+        ("solutions", ctypes.c_uint64),
+        ("nodes", ctypes.c_uint64),
+        ("subtrees", ctypes.c_uint64),
+        ("expansion_nodes", ctypes.c_uint64),
+        ("status", ctypes.c_int32),
+        ("split_depth", ctypes.c_uint32),
+        ("has_first_solution", ctypes.c_uint32),
+        ("first_solution", ctypes.c_uint32 * 256),
+        ("kernel_ms", ctypes.c_double),
+        ("total_ms", ctypes.c_double),
+        ("rounds", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32),
+    ]
+
+
+# name -> (restype, argtypes); every symbol declared in include/emp_b200.h
+SIGNATURES = {
+    "emp_abi_version": (ctypes.c_uint32, []),
+    "emp_last_error": (ctypes.c_char_p, []),
+    "emp_generate_puzzle": (ctypes.c_int32, [ctypes.c_uint32] * 4 + [ctypes.c_uint64, u8p]),
+    "emp_puzzle_create": (ctypes.c_int32, [ctypes.POINTER(PuzzleDesc), ctypes.POINTER(ctypes.c_void_p)]),
+    "emp_puzzle_destroy": (None, [ctypes.c_void_p]),
+    "emp_puzzle_get_info": (ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(PuzzleInfo)]),
+    "emp_puzzle_export_tables": (ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint32), ctypes.c_uint64,
+                                                  u64p]),
+    "emp_bt_count": (ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(BtConfig), ctypes.POINTER(BtResult)]),
+    "emp_bt_count_batch": (ctypes.c_int32, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_uint32, ctypes.POINTER(BtConfig),
+                                            ctypes.POINTER(BtResult)]),
+    "emp_bt_plan_create": (ctypes.c_int32, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_uint32, ctypes.POINTER(BtConfig),
+                                            ctypes.POINTER(ctypes.c_void_p)]),
+    "emp_bt_plan_subtrees": (ctypes.c_int32, [ctypes.c_void_p, u64p]),
+    "emp_bt_plan_select": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64]),
+    "emp_bt_plan_run": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_void_p]),
+    "emp_bt_plan_results": (ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(BtResult)]),
+    "emp_bt_plan_subtree_counts": (ctypes.c_int32, [ctypes.c_void_p, u64p, u64p, ctypes.c_uint64]),
+    "emp_bt_plan_subtree_prefix": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_uint64, u16p, ctypes.c_uint32]),
+    "emp_bt_plan_destroy": (None, [ctypes.c_void_p]),
+}
+
+_lib = None
+
+
+def load():
+    """Load libemp_b200.so (raises when it is missing: there is no fallback)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing; build it with python -m edge_matching_puzzle_b200.build")
+        lib = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+    return _lib
+
+
+def check(status: int) -> int:
+    if status < 0:
+        raise EmpError(status, load().emp_last_error().decode())
+    return status
+
+
+def generate(width: int, height: int, border_colors: int, interior_colors: int, seed: int) -> List[List[int]]:
+    buf = (ctypes.c_uint8 * (4 * width * height))()
+    check(load().emp_generate_puzzle(width, height, border_colors, interior_colors, seed, buf))
+    raw = list(buf)
+    return [raw[4 * i:4 * i + 4] for i in range(width * height)]
+
+
+class NativePuzzle:
+    """Owns an emp_puzzle handle."""
+
+    def __init__(self, width: int, height: int, colors: Sequence[Sequence[int]], order: Optional[Sequence[int]] = None):
+        L = load()
+        n = width * height
+        self._colours = (ctypes.c_uint8 * (4 * n))(*[c for p in colors for c in p])
+        self._order = (ctypes.c_uint16 * n)(*order) if order is not None else None
+        desc = PuzzleDesc(width, height, ctypes.cast(self._colours, u8p),
+                          ctypes.cast(self._order, u16p) if self._order is not None else None)
+        h = ctypes.c_void_p()
+        check(L.emp_puzzle_create(ctypes.byref(desc), ctypes.byref(h)))
+        self.handle = h
+        self.width, self.height, self.n = width, height, n
+
+    def close(self):
+        if getattr(self, "handle", None):
+            load().emp_puzzle_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        self.close()
+
+    def export_tables(self) -> List[int]:
+        words = ctypes.c_uint64()
+        check(load().emp_puzzle_export_tables(self.handle, None, 0, ctypes.byref(words)))
+        buf = (ctypes.c_uint32 * words.value)()
+        check(load().emp_puzzle_export_tables(self.handle, buf, words.value, ctypes.byref(words)))
+        return list(buf)
+
+    def info(self) -> PuzzleInfo:
+        i = PuzzleInfo()
+        check(load().emp_puzzle_get_info(self.handle, ctypes.byref(i)))
+        return i
+
+
+def bt_config(**kw) -> BtConfig:
+    c = BtConfig()
+    c.device = -1
+    for k, v in kw.items():
+        setattr(c, k, v)
+    return c
+
+
+def bt_count(puzzle: NativePuzzle, **kw) -> BtResult:
+    r = BtResult()
+    cfg = bt_config(**kw)
+    check(load().emp_bt_count(puzzle.handle, ctypes.byref(cfg), ctypes.byref(r)))
+    return r
+
+
+def bt_count_batch(puzzles: Sequence[NativePuzzle], **kw) -> List[BtResult]:
+    arr = (ctypes.c_void_p * len(puzzles))(*[p.handle for p in puzzles])
+    res = (BtResult * len(puzzles))()
+    cfg = bt_config(**kw)
+    check(load().emp_bt_count_batch(arr, len(puzzles), ctypes.byref(cfg), res))
+    return list(res)
+
+
+class BtPlan:
+    """emp_bt_plan: prefix expansion done once, kernel runs on demand."""
+
+    def __init__(self, puzzles: Sequence[NativePuzzle], **kw):
+        self.puzzles = list(puzzles)
+        arr = (ctypes.c_void_p * len(puzzles))(*[p.handle for p in puzzles])
+        self.cfg = bt_config(**kw)
+        h = ctypes.c_void_p()
+        check(load().emp_bt_plan_create(arr, len(puzzles), ctypes.byref(self.cfg), ctypes.byref(h)))
+        self.handle = h
+        self.selected = None
+
+    def subtrees(self) -> int:
+        n = ctypes.c_uint64()
+        check(load().emp_bt_plan_subtrees(self.handle, ctypes.byref(n)))
+        return n.value
+
+    def select(self, first: int, stride: int, count: int) -> None:
+        check(load().emp_bt_plan_select(self.handle, first, stride, count))
+        self.selected = count
+
+    def run(self, stream: int = 0) -> None:
+        check(load().emp_bt_plan_run(self.handle, ctypes.c_void_p(stream) if stream else None))
+
+    def results(self) -> List[BtResult]:
+        res = (BtResult * len(self.puzzles))()
+        check(load().emp_bt_plan_results(self.handle, res))
+        return list(res)
+
+    def subtree_counts(self, count: int):
+        nn = (ctypes.c_uint64 * count)()
+        ss = (ctypes.c_uint64 * count)()
+        check(load().emp_bt_plan_subtree_counts(self.handle, nn, ss, count))
+        return list(nn), list(ss)
+
+    def subtree_prefix(self, index: int, depth: int) -> List[int]:
+        buf = (ctypes.c_uint16 * depth)()
+        check(load().emp_bt_plan_subtree_prefix(self.handle, index, buf, depth))
+        return list(buf)
+
+    def close(self):
+        if getattr(self, "handle", None):
+            load().emp_bt_plan_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        self.close()

@@ -1,0 +1,160 @@
+/*
+ * edge_matching_puzzle_b200 -- C ABI of the B200 search library.
+ *
+ * This is the boundary the reference's feature plugins call into.  In the
+ * reference, feature_CUDA_backtracker::run (src/feature_CUDA_backtracker.cpp:
+ * 31-38) calls
+ *     void launch_CUDA_backtracker(const emp_piece_db&, const emp_FSM_info&,
+ *                                  const emp_variable_generator&,
+ *                                  const emp_strategy_generator&);
+ * (include/feature_CUDA_backtracker.h:68-72) and feature_CUDA_glutton_max::run
+ * (include/feature_CUDA_glutton_max.h:72-75) calls
+ *     void launch_CUDA_glutton_max(const emp_piece_db&, const emp_FSM_info&);
+ * (include/feature_CUDA_glutton_max.h:55-57).  Both launchers take the piece
+ * database and the puzzle geometry; here those are flattened into
+ * emp_puzzle_desc (piece colours + position order), and the results the
+ * reference only prints are returned in plain structs.  The C++ launchers in
+ * edge_matching_puzzle_b200/csrc/host keep the reference signatures and print
+ * the reference's lines on top of this ABI.
+ *
+ * Rules: plain pointers and sizes only; no exception crosses the boundary;
+ * every call returns an emp_status and emp_last_error() describes the last
+ * failure of the calling thread.  A handle may be used by one call at a time.
+ */
+#ifndef EMP_B200_H
+#define EMP_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define EMP_ABI_VERSION 1u
+
+typedef int32_t emp_status;
+#define EMP_OK 0
+#define EMP_INCOMPLETE 1          /* stopped by the timeout or a cancel: partial counts */
+#define EMP_ERR_INVALID (-1)      /* bad argument or malformed puzzle */
+#define EMP_ERR_UNSUPPORTED (-2)  /* valid input outside what the kernels support */
+#define EMP_ERR_CUDA (-3)         /* CUDA runtime error (no device, launch failure...) */
+#define EMP_ERR_NOMEM (-4)        /* device allocation failed */
+
+/* Version of this ABI (EMP_ABI_VERSION). */
+uint32_t emp_abi_version(void);
+
+/* Message of the last failing call on this thread ("" when none). */
+const char *emp_last_error(void);
+
+/* Seeded puzzle generator of the project's workloads (splitmix64 stream):
+ * frame-to-frame edges get colours 1..border_colors, other internal edges
+ * border_colors+1..border_colors+interior_colors, outer edges 0; pieces are
+ * shuffled and rotated.  colours_out receives 4*w*h bytes (N,E,S,W per piece).
+ * Replaces the hand-written puzzle files of doc/example (no counterpart
+ * function in the reference). */
+emp_status emp_generate_puzzle(uint32_t width, uint32_t height, uint32_t border_colors,
+                               uint32_t interior_colors, uint64_t seed, uint8_t *colours_out);
+
+/* Puzzle description: what emp_pieces_parser::parse (include/emp_pieces_parser.h:
+ * 53-101) and emp_strategy_generator (include/emp_strategy_generator.h:161-184)
+ * provide to the reference's launchers. */
+typedef struct emp_puzzle_desc {
+    uint32_t width;
+    uint32_t height;
+    const uint8_t *colours;   /* 4*width*height bytes: N,E,S,W of piece id i+1; 0 = frame */
+    const uint16_t *order;    /* width*height positions y*width+x in visiting order;
+                                 NULL = row-major ("basic" strategy) */
+} emp_puzzle_desc;
+
+typedef struct emp_puzzle_t *emp_puzzle;
+
+/* Builds the piece database (kinds, identical pieces, colour masks) and the
+ * level plan of the order, as emp_piece_db's constructor (include/
+ * emp_piece_db.h:466-1170) and emp_strategy's constructor (include/
+ * emp_strategy.h:159-265) do.  Fails with EMP_ERR_INVALID on the inputs the
+ * reference rejects (wrong kind counts, odd colour counts) and with
+ * EMP_ERR_UNSUPPORTED beyond 256 pieces or colour id 30. */
+emp_status emp_puzzle_create(const emp_puzzle_desc *desc, emp_puzzle *out);
+void emp_puzzle_destroy(emp_puzzle puzzle);
+
+typedef struct emp_puzzle_info {
+    uint32_t width, height, nb_pieces;
+    uint32_t nb_center, nb_border, nb_corner;
+    uint32_t border_color_id;     /* max colour id + 1 (emp_piece_db.h:620) */
+    uint32_t has_identical;       /* the reference needs HANDLE_IDENTICAL_PIECES */
+    uint32_t identical_masks_with_extra;  /* transitions whose identical mask clears other candidates */
+} emp_puzzle_info;
+
+emp_status emp_puzzle_get_info(emp_puzzle puzzle, emp_puzzle_info *info);
+
+/* Copies the puzzle's GPU table blob (header, per-side colour masks, level
+ * plan, identical masks; layout in edge_matching_puzzle_b200/csrc/emp_model.h)
+ * to out when capacity suffices; *words receives its size in 32-bit words.
+ * Introspection for tests: no counterpart in the reference. */
+emp_status emp_puzzle_export_tables(emp_puzzle puzzle, uint32_t *out, uint64_t capacity, uint64_t *words);
+
+/* ---------------- exhaustive backtracker (emp_strategy semantics) ---------------- */
+
+typedef struct emp_bt_config {
+    uint32_t split_depth;        /* levels expanded before subtrees go to threads; 0 = auto */
+    uint32_t threads_per_block;  /* 0 = auto (autotuner cache or default) */
+    uint32_t blocks_per_sm;      /* 0 = as many as fit */
+    uint32_t stop_at_first;      /* 1: stop once the reference's first solution is known */
+    uint64_t reserved_budget;    /* unused, keep 0 */
+    uint32_t timeout_ms;         /* kernel deadline; 0 = none */
+    int32_t device;              /* CUDA device ordinal; -1 = current device */
+    uint32_t keep_subtree_counts;/* 1: keep per-subtree counts for emp_bt_plan_subtree_counts */
+    uint32_t split_budget;       /* DFS steps a thread spends on a work record before handing the
+                                    rest back as new records; 0 = default (32768) */
+    uint32_t reserved[6];
+} emp_bt_config;
+
+typedef struct emp_bt_result {
+    uint64_t solutions;          /* "Nb solutions" (include/emp_strategy.h:413) */
+    uint64_t nodes;              /* "Total situations explored" (:412) */
+    uint64_t subtrees;           /* prefixes at the split depth */
+    uint64_t expansion_nodes;    /* placements at levels below the split depth */
+    int32_t status;              /* EMP_OK or EMP_INCOMPLETE */
+    uint32_t split_depth;
+    uint32_t has_first_solution;
+    uint32_t first_solution[256];/* per board position y*w+x: (piece id-1)<<2 | orientation */
+    double kernel_ms;            /* DFS kernel time (device events, all rounds) */
+    double total_ms;             /* whole call, host clock */
+    uint32_t rounds;             /* DFS rounds (work handed back between rounds) */
+    uint32_t reserved;
+} emp_bt_result;
+
+/* Exhaustive count of one puzzle: every solution and every placement of the
+ * reference's search (position 0 keeps its first candidate, emp_strategy.h:389). */
+emp_status emp_bt_count(emp_puzzle puzzle, const emp_bt_config *config, emp_bt_result *result);
+
+/* Same for many puzzles in one persistent launch; results[i] per puzzle. */
+emp_status emp_bt_count_batch(const emp_puzzle *puzzles, uint32_t count, const emp_bt_config *config,
+                              emp_bt_result *results);
+
+/* Split form of the batch call: plan (upload + prefix expansion), run (kernel
+ * launch on a stream, asynchronous), results (synchronise + download). */
+typedef struct emp_bt_plan_t *emp_bt_plan;
+
+emp_status emp_bt_plan_create(const emp_puzzle *puzzles, uint32_t count, const emp_bt_config *config,
+                              emp_bt_plan *out);
+/* Number of subtrees of the plan (all puzzles). */
+emp_status emp_bt_plan_subtrees(emp_bt_plan plan, uint64_t *subtrees);
+/* Restrict the next runs to subtrees first, first+stride, ... (count of them). */
+emp_status emp_bt_plan_select(emp_bt_plan plan, uint64_t first, uint64_t stride, uint64_t count);
+/* Launch on stream (a cudaStream_t; NULL = default stream). */
+emp_status emp_bt_plan_run(emp_bt_plan plan, void *stream);
+/* Wait for the last run and fill results[count] (per puzzle). */
+emp_status emp_bt_plan_results(emp_bt_plan plan, emp_bt_result *results);
+/* Per-subtree counts of the last run in selection order (needs keep_subtree_counts). */
+emp_status emp_bt_plan_subtree_counts(emp_bt_plan plan, uint64_t *nodes, uint64_t *solutions,
+                                      uint64_t capacity);
+/* Prefix (split_depth transitions t = kind_index<<2|orientation) of a selected subtree. */
+emp_status emp_bt_plan_subtree_prefix(emp_bt_plan plan, uint64_t index, uint16_t *prefix, uint32_t capacity);
+void emp_bt_plan_destroy(emp_bt_plan plan);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* EMP_B200_H */

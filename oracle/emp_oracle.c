@@ -636,6 +636,55 @@ uint64_t op_bt_expand(op_puzzle *p, const uint32_t *order, uint32_t depth, uint1
     return count;
 }
 
+
+/* Knuth's random-probe estimate of the exhaustive tree size (placements):
+ * E[prod of branching factors] summed over levels.  Used only to size
+ * workloads; it does not take part in any parity check. */
+double op_bt_estimate(op_puzzle *p, const uint32_t *order, uint32_t probes, uint64_t seed,
+                      double *per_level)
+{
+    build_table(p);
+    bt_state s;
+    bt_init(&s, p, order);
+    uint32_t n = s.n;
+    double total = 0;
+    uint64_t x = seed * 0x9E3779B97F4A7C15ull + 1;
+    for (uint32_t pr = 0; pr < probes; ++pr) {
+        double weight = 1;
+        for (uint32_t i = 0; i < n; ++i) s.piece_info[i] = 0;
+        uint32_t idx = 0;
+        bt_compute(&s, 0);
+        for (;;) {
+            /* candidates actually tried at this level (identical masks applied in order) */
+            uint32_t cand[1024], nc = 0;
+            uint64_t *at = s.avail_trans + (size_t)idx * s.maxw;
+            uint64_t save[16];
+            memcpy(save, at, sizeof(uint64_t) * s.maxw);
+            uint32_t t1;
+            while ((t1 = bt_next(&s, idx)) != 0) {
+                cand[nc++] = t1 - 1;
+                bt_select(&s, idx, t1 - 1);
+                if (idx == 0) break;   /* position 0 keeps its first transition */
+            }
+            memcpy(at, save, sizeof(uint64_t) * s.maxw);
+            if (!nc) break;
+            weight *= nc;
+            total += weight;
+            if (per_level) per_level[idx] += weight;
+            x ^= x << 13; x ^= x >> 7; x ^= x << 17;
+            uint32_t t = cand[x % nc];
+            s.piece_info[idx] = p->binary[s.kind[idx]][t];
+            bt_select(&s, idx, t);
+            ++idx;
+            if (idx == n) break;
+            bt_compute(&s, idx);
+        }
+    }
+    bt_free(&s);
+    if (per_level) for (uint32_t i = 0; i < n; ++i) per_level[i] /= probes;
+    return total / probes;
+}
+
 typedef struct {
     op_puzzle *p;
     const uint32_t *order;

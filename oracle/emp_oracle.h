@@ -105,6 +105,10 @@ int op_bt_subtrees_parallel(op_puzzle *p, const uint32_t *order,
                             uint64_t *nodes, uint64_t *solutions,
                             uint64_t *per_nodes, uint64_t *per_solutions);
 
+/* Knuth random-probe estimate of the exhaustive tree size (sizing only). */
+double op_bt_estimate(op_puzzle *p, const uint32_t *order, uint32_t probes,
+                      uint64_t seed, double *per_level);
+
 typedef struct {
     uint64_t placements;   /* trial evaluations + committed pushes */
     uint32_t max_level;    /* best number of pieces placed (m_max) */

@@ -1,0 +1,147 @@
+"""GPU parity of the exhaustive backtracker against the CPU oracle (bit-exact counts).
+
+The CUDA path is reached through the C ABI (libemp_b200.so); the oracle is the judge.
+"""
+from __future__ import annotations
+
+import random
+
+import pytest
+
+from edge_matching_puzzle_b200 import native
+from edge_matching_puzzle_b200.puzzle import Puzzle, board_string, generate, spiral_order
+from oracle.oracle import OraclePuzzle
+
+pytestmark = pytest.mark.gpu
+
+
+def _check(pz: Puzzle, order=None, depths=(None,), **kw):
+    op = OraclePuzzle(pz.width, pz.height, pz.colors)
+    want, _ = op.run(order=order)
+    npz = native.NativePuzzle(pz.width, pz.height, pz.colors, order=order)
+    for d in depths:
+        r = native.bt_count(npz, split_depth=d or 0, **kw)
+        assert r.status == native.EMP_OK
+        assert (r.nodes, r.solutions) == (want.nodes, want.solutions), (d, r.nodes, want.nodes)
+        if want.solutions:
+            assert r.has_first_solution
+            assert list(r.first_solution)[: pz.nb_pieces] == list(want.first_board)[: pz.nb_pieces]
+        else:
+            assert not r.has_first_solution
+    return want
+
+
+@pytest.mark.parametrize("name", ["3_3", "4_4", "5_5", "5_5_bis"])
+def test_reference_examples_row_major(reference_vectors, name):
+    pz = Puzzle.from_csv(reference_vectors["puzzles"][name])
+    _check(pz, depths=(1, 2, 4, pz.nb_pieces - 1))
+
+
+@pytest.mark.parametrize("name", ["3_3", "4_4", "5_5"])
+def test_reference_examples_spiral(reference_vectors, name):
+    """The spiral order reproduces the reference's golden counts 37/3284/37938."""
+    pz = Puzzle.from_csv(reference_vectors["puzzles"][name])
+    want = _check(pz, order=spiral_order(pz.width, pz.height), depths=(1, 3, pz.nb_pieces - 1))
+    assert (want.nodes, want.solutions) == {"3_3": (37, 2), "4_4": (3284, 12), "5_5": (37938, 1)}[name]
+
+
+def test_backtracker_first_solution_golden(reference_vectors):
+    for name in ("3_3", "4_4", "5_5"):
+        pz = Puzzle.from_csv(reference_vectors["puzzles"][name])
+        r = native.bt_count(native.NativePuzzle(pz.width, pz.height, pz.colors), stop_at_first=1)
+        board = board_string(pz.width, pz.height, list(r.first_solution))
+        assert board == reference_vectors["backtracker_first_solution"][name]
+
+
+@pytest.mark.parametrize("seed", [0, 1, 2, 3])
+def test_config0_counts(config_counts, seed):
+    rec = [r for r in config_counts["records"] if r["config"] == "5x5" and r["seed"] == seed][0]
+    pz = generate(5, 5, 3, 5, seed)
+    r = native.bt_count(native.NativePuzzle(5, 5, pz.colors), split_depth=12)
+    assert (r.nodes, r.solutions) == (rec["nodes"], rec["solutions"])
+    assert r.has_first_solution
+
+
+@pytest.mark.parametrize("seed", range(24))
+def test_random_small_puzzles(seed):
+    """Mixed shapes and colour counts, including puzzles whose identical-piece masks
+    clear unrelated candidates (half-symmetric pieces), against the oracle."""
+    rng = random.Random(1000 + seed)
+    while True:  # draw until the tree is small enough for the oracle (a few seconds)
+        w, h = rng.randint(3, 6), rng.randint(3, 6)
+        pz = generate(w, h, rng.randint(1, 3), rng.randint(2, 5), rng.randint(0, 1 << 30))
+        if OraclePuzzle(w, h, pz.colors).estimate(2000) < 3e6:
+            break
+    _check(pz, depths=(1, min(5, w * h - 1), w * h - 1), split_budget=rng.choice([0, 256]))
+
+
+def test_quirky_identical_masks_present():
+    """At least one workload puzzle exercises identical masks with extra clears."""
+    found = 0
+    for seed in range(16):
+        pz = generate(8, 8, 4, 8, seed)
+        found += native.NativePuzzle(8, 8, pz.colors).info().identical_masks_with_extra > 0
+    assert found >= 1
+
+
+def test_8x8_subtree_parity_sample():  # noqa: D103
+    """Per-subtree node and solution counts of an 8x8 workload puzzle against the oracle."""
+    pz = generate(8, 8, 4, 8, 5)  # seed with identical masks that clear extra candidates
+    npz = native.NativePuzzle(8, 8, pz.colors)
+    assert npz.info().identical_masks_with_extra > 0
+    op = OraclePuzzle(8, 8, pz.colors)
+    depth = 18
+    plan = native.BtPlan([npz], split_depth=depth, keep_subtree_counts=1, split_budget=512, timeout_ms=60000)
+    total = plan.subtrees()
+    count, _, _, _ = op.expand(depth)
+    assert total == count
+    sample = 1500
+    stride = max(1, total // sample)
+    plan.select(7, stride, sample)
+    plan.run()
+    res = plan.results()[0]
+    nodes, sols = plan.subtree_counts(sample)
+    for i in range(0, sample, 7):
+        prefix = plan.subtree_prefix(i, depth)
+        want_n, want_s, st = op.subtree(prefix)
+        assert (nodes[i], sols[i]) == (want_n, want_s), i
+    assert res.nodes == sum(nodes) and res.solutions == sum(sols)
+
+
+def test_8x8_full_count_against_cpu_golden(config_counts):
+    """Whole exhaustive count of an 8x8 workload seed equals the CPU oracle's count."""
+    recs = [r for r in config_counts["records"] if r["config"] == "8x8"]
+    rec = min(recs, key=lambda r: r["nodes"])
+    pz = generate(8, 8, 4, 8, rec["seed"])
+    r = native.bt_count(native.NativePuzzle(8, 8, pz.colors), split_depth=12, timeout_ms=60000)
+    assert r.status == native.EMP_OK
+    assert (r.nodes, r.solutions) == (rec["nodes"], rec["solutions"])
+
+
+def test_split_depth_invariance():
+    pz = generate(6, 6, 3, 4, 11)
+    npz = native.NativePuzzle(6, 6, pz.colors)
+    got = {d: (lambda r: (r.nodes, r.solutions))(native.bt_count(npz, split_depth=d)) for d in (1, 6, 12, 20, 35)}
+    assert len(set(got.values())) == 1
+
+
+@pytest.mark.parametrize("budget", [64, 1024, 1 << 20])
+def test_split_budget_invariance(budget):
+    """Handing work back between rounds (small budgets: many rounds) changes nothing."""
+    pz = generate(6, 6, 3, 4, 5)
+    want = _check(pz, depths=(6,), split_budget=budget)
+    r = native.bt_count(native.NativePuzzle(6, 6, pz.colors), split_depth=6, split_budget=budget)
+    assert r.nodes == want.nodes
+    if budget == 64:
+        assert r.rounds > 1
+
+
+def test_timeout_stops_kernel():
+    pz = generate(8, 8, 4, 8, 13)  # the largest tree of the workload
+    npz = native.NativePuzzle(8, 8, pz.colors)
+    import ctypes
+    cfg = native.bt_config(split_depth=12, timeout_ms=200)
+    r = native.BtResult()
+    st = native.load().emp_bt_count(npz.handle, ctypes.byref(cfg), ctypes.byref(r))
+    assert st == native.EMP_INCOMPLETE
+    assert r.kernel_ms < 5000
