@@ -54,7 +54,7 @@ extern "C" emp_status emp_puzzle_create(const emp_puzzle_desc* desc, emp_puzzle*
     emp::build_device_tables(p->model, p->plan, p->tables);
     for (uint32_t k = 0; k < 3; ++k)
         for (uint32_t e = 0; e < 4 * p->model.nb_kind(k); ++e)
-            p->extra_count += (p->tables.blob[p->tables.tinfo_kind_off[k] + e] >> 20) & 1u;
+            p->extra_count += (p->tables.blob[p->tables.tinfo_off[k] + e] >> 20) & 1u;
     *out = p.release();
     return EMP_OK;
 }
@@ -124,9 +124,9 @@ struct emp_bt_plan_t {
         P.max_levels = max_levels;
         P.max_avail_words = max_avail;
         P.max_kw = max_kw;
-        P.spill = spill.as<uint32_t>();
+        P.spill = spill.as<uint64_t>();
         P.rec_words = rec_words;
-        P.rec_r_off = rec_words - max_kw;
+        P.rec_r_off = rec_words - 2 * max_kw;
         P.out_capacity = capacity;
         P.item_budget = budget;
         unsigned long long* c = counters.as<unsigned long long>();
@@ -241,7 +241,7 @@ extern "C" emp_status emp_bt_plan_create(const emp_puzzle* puzzles, uint32_t cou
         min_n = std::min(min_n, t.n);
         pl->max_levels = std::max(pl->max_levels, t.n);
         pl->max_avail = std::max(pl->max_avail, t.avail_words);
-        for (uint32_t k = 0; k < 3; ++k) pl->max_kw = std::max(pl->max_kw, t.kw[k]);
+        pl->max_kw = std::max(pl->max_kw, t.max_kw);
     }
     pl->depth = pl->cfg.split_depth ? pl->cfg.split_depth : auto_depth(min_n);
     if (pl->depth >= min_n || pl->depth > 64)
@@ -252,7 +252,7 @@ extern "C" emp_status emp_bt_plan_create(const emp_puzzle* puzzles, uint32_t cou
     std::vector<uint32_t> blob;
     std::vector<uint64_t> offs;
     for (emp_puzzle p : pl->puzzles) {
-        offs.push_back(blob.size());
+        offs.push_back(blob.size());  // blobs are multiples of 4 words: 16-byte aligned tables
         blob.insert(blob.end(), p->tables.blob.begin(), p->tables.blob.end());
     }
     CUDA_TRY(pl->tables.alloc(sizeof(uint32_t) * blob.size()));
@@ -277,15 +277,15 @@ extern "C" emp_status emp_bt_plan_create(const emp_puzzle* puzzles, uint32_t cou
     const size_t smem = emp::dfs_smem_bytes(pl->max_levels, pl->max_avail, pl->threads);
     if (smem > static_cast<size_t>(prop.sharedMemPerBlockOptin))
         return fail(EMP_ERR_UNSUPPORTED, "per-thread DFS state does not fit shared memory; use fewer threads per block");
-    CUDA_TRY(cudaFuncSetAttribute(emp::dfs_kernel_symbol(), cudaFuncAttributeMaxDynamicSharedMemorySize,
+    CUDA_TRY(cudaFuncSetAttribute(emp::dfs_kernel_symbol(pl->max_kw), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   static_cast<int>(smem)));
     int per_sm = 0;
-    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, emp::dfs_kernel_symbol(),
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, emp::dfs_kernel_symbol(pl->max_kw),
                                                            static_cast<int>(pl->threads), smem));
     if (per_sm < 1) return fail(EMP_ERR_UNSUPPORTED, "DFS kernel cannot be resident with this configuration");
     if (pl->cfg.blocks_per_sm) per_sm = std::min<int>(per_sm, static_cast<int>(pl->cfg.blocks_per_sm));
     pl->blocks = static_cast<uint32_t>(per_sm) * static_cast<uint32_t>(prop.multiProcessorCount);
-    CUDA_TRY(pl->spill.alloc(sizeof(uint32_t) * static_cast<size_t>(pl->blocks) * pl->threads * pl->max_levels *
+    CUDA_TRY(pl->spill.alloc(sizeof(uint64_t) * static_cast<size_t>(pl->blocks) * pl->threads * pl->max_levels *
                              pl->max_kw));
     // round queues: room for every resident thread to hand back a full path twice
     const uint64_t resident = static_cast<uint64_t>(pl->blocks) * pl->threads;
@@ -293,7 +293,7 @@ extern "C" emp_status emp_bt_plan_create(const emp_puzzle* puzzles, uint32_t cou
     pl->capacity = std::min<uint64_t>(pl->capacity, (uint64_t)1 << 23);
     CUDA_TRY(pl->rec_a.alloc(sizeof(uint32_t) * pl->rec_words * pl->capacity));
     CUDA_TRY(pl->rec_b.alloc(sizeof(uint32_t) * pl->rec_words * pl->capacity));
-    pl->budget = pl->cfg.split_budget ? pl->cfg.split_budget : (1u << 15);
+    pl->budget = pl->cfg.split_budget ? pl->cfg.split_budget : 2048u;
     EMP_TRY(build_initial(*pl, 0, 1, pl->n_all));
     *out = pl.release();
     return EMP_OK;

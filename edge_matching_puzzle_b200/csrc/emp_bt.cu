@@ -34,7 +34,8 @@ namespace {
 
 constexpr unsigned kFull = 0xFFFFFFFFu;
 constexpr uint32_t kMaxExpandDepth = 64;
-constexpr uint32_t kMaxAvailWords = 96;
+constexpr uint32_t kMaxAvailWords = 24;   // 64-bit availability words, three kinds
+constexpr uint32_t kMaxKindWords = 16;    // 64-bit words of one kind (256 pieces)
 
 __device__ __forceinline__ uint64_t global_ns()
 {
@@ -56,39 +57,40 @@ __global__ void expand_kernel(BtLaunch P, const uint16_t* __restrict__ parents,
          i += (uint64_t)gridDim.x * blockDim.x) {
         const uint32_t pz = parent_puzzle ? parent_puzzle[i] : 0u;
         const uint32_t* tb = P.tables + P.puzzle_offset[pz];
-        const uint32_t n = ldg(tb + H_N), ncol = ldg(tb + H_NCOL);
-        uint32_t av[kMaxAvailWords];
-        uint32_t cols[kMaxExpandDepth];
-        const uint32_t aw = ldg(tb + H_AWORDS);
-        for (uint32_t w = 0; w < aw; ++w) av[w] = ldg(tb + ldg(tb + H_INIT) + w);
+        const uint32_t n = ldg(tb + H_N), ncol = ldg(tb + H_NCOL), desc_off = ldg(tb + H_DESC);
+        uint64_t av[kMaxAvailWords];
+        uint32_t stk[kMaxExpandDepth];
+        const uint32_t aw = ldg(tb + H_AWORDS), init = ldg(tb + H_INIT);
+        for (uint32_t w = 0; w < aw; ++w) av[w] = ldg64(tb + init + 2 * w);
         const uint16_t* pre = parents + i * level;
         for (uint32_t l = 0; l < level; ++l) {
-            const LevelDesc d = load_desc(tb, l);
+            const LevelDesc d = load_desc(tb, desc_off, l);
             const uint32_t t = pre[l];
-            av[d.aoff + (t >> 5)] &= ~(0xFu << (t & 28u));
-            cols[l] = ldg(tb + ldg(tb + H_TINFO + d.kind) + t) & 0xFFFFFu;
+            av[d.aoff() + (t >> 6)] &= ~(0xFull << (t & 60u));
+            stk[l] = ldg(tb + d.d5 + t) & 0xFFFFFu;
         }
         uint32_t cnt = 0;
         if (level < n) {
-            const LevelDesc d = load_desc(tb, level);
-            const uint32_t* sm[4];
-            for (uint32_t j = 0; j < d.nplaced; ++j) {
-                const uint32_t s = desc_side(d, j);
-                const uint32_t c = (cols[desc_nb(d, j)] >> (5 * ((s + 2) & 3))) & 31u;
-                sm[j] = tb + ldg(tb + H_SIDE + d.kind) + (s * ncol + c) * d.kw;
+            const LevelDesc d = load_desc(tb, desc_off, level);
+            const uint32_t kw = d.kw();
+            uint32_t row = d.d2;
+            if (d.arity() >= 1) {
+                const uint32_t ca = facing_colour(stk[d.level_a()], d.side_a());
+                const uint32_t cb = d.arity() >= 2 ? facing_colour(stk[d.level_b()], d.side_b()) : 0u;
+                row += ((d.arity() >= 2 ? ca * ncol + cb : ca) * kw) * 2;
             }
-            uint32_t R[32];
-            for (uint32_t w = 0; w < d.kw; ++w) {
-                uint32_t x = ldg(tb + d.base + w) & av[d.aoff + w];
-                for (uint32_t j = 0; j < d.nplaced; ++j) x &= ldg(sm[j] + w);
-                R[w] = x;
+            uint64_t R[kMaxKindWords];
+            for (uint32_t w = 0; w < kw; ++w) R[w] = ldg64(tb + row + 2 * w) & av[d.aoff() + w];
+            for (uint32_t j = 0; j < d.nextra(); ++j) {
+                const uint32_t sd = d.extra_side(j);
+                const uint32_t c = facing_colour(stk[d.extra_level(j)], sd);
+                const uint32_t* sm = tb + d.d4 + ((sd * ncol + c) * kw) * 2;
+                for (uint32_t w = 0; w < kw; ++w) R[w] &= ldg64(sm + 2 * w);
             }
-            const uint32_t* extra = tb + ldg(tb + H_EXTRA + d.kind);
-            const uint32_t* tinfo = tb + ldg(tb + H_TINFO + d.kind);
             uint64_t out = mode ? offsets[i] : 0;
-            for (uint32_t w = 0; w < d.kw; ++w) {
+            for (uint32_t w = 0; w < kw; ++w) {
                 while (R[w]) {
-                    const uint32_t t = w * 32 + __ffs(R[w]) - 1;
+                    const uint32_t t = w * 64 + __ffsll(R[w]) - 1;
                     if (mode) {
                         uint16_t* c = children + out * (level + 1);
                         for (uint32_t l = 0; l < level; ++l) c[l] = pre[l];
@@ -97,11 +99,15 @@ __global__ void expand_kernel(BtLaunch P, const uint16_t* __restrict__ parents,
                         ++out;
                     }
                     ++cnt;
-                    if (level == 0) { R[w] = 0; w = d.kw; break; }  // position 0 keeps its first transition
-                    if ((ldg(tinfo + t) >> 20) & 1u) {
-                        for (uint32_t ww = 0; ww < d.kw; ++ww) R[ww] &= ldg(extra + t * d.kw + ww);
+                    if (level == 0) {  // position 0 keeps its first transition (emp_strategy.h:389)
+                        w = kw;
+                        break;
+                    }
+                    if ((ldg(tb + d.d5 + t) >> 20) & 1u) {
+                        const uint32_t* ex = tb + d.d6 + t * kw * 2;
+                        for (uint32_t ww = 0; ww < kw; ++ww) R[ww] &= ldg64(ex + 2 * ww);
                     } else {
-                        R[w] &= ~(1u << (t & 31));
+                        R[w] &= ~(1ull << (t & 63));
                     }
                 }
             }
@@ -185,19 +191,25 @@ __global__ void scan_apply(const uint32_t* __restrict__ in, uint64_t n, const ui
 //
 // A work record is "prefix t[0..len-1], resume bit `start` at level len"
 // (plus the exact remaining set of level len when it is spilled).  The initial
-// records are the split-depth prefixes with start 0.  A thread that spends
-// more than `item_budget` steps on a record hands its remaining work back as
-// one record per level that still has candidates (the current level from its
-// resume bit, every shallower level from its next sibling) for the next round,
-// so a huge subtree spreads over the GPU in a few rounds.
+// records are the split-depth prefixes with start 0.  Once a round's queue is
+// empty, a thread that spent more than `item_budget` steps on its record hands
+// the remaining work back as one record per level that still has candidates
+// (the current level from its resume bit, every shallower level from its next
+// sibling) for the next round, so a huge subtree spreads over the GPU in a few
+// rounds.
 //
 // record words: [0,1] subtree id (for per-subtree counts), [2] len | start<<16,
 // [3] puzzle | spilled<<16 | empty<<17, [4..] transitions (u16 pairs), then
-// the remaining set of level len (max_kw words).
+// the remaining set of level len (max_kw 64-bit words as u32 pairs).
+//
+// Per-thread state in shared memory, thread-interleaved (a warp touching its
+// own entries hits distinct banks):
+//   stk[L*T + tid] = t << 21 | spilled << 20 | colours of the placed piece
+//   av[w*T + tid]  = 64-bit availability words of the three kinds
 struct ThreadItem {
     uint64_t orig;
     const uint32_t* tb;
-    uint32_t pz, n, ncol, L, base, start, spilled;
+    uint32_t pz, n, ncol, desc_off, L, base, start, spilled;
     uint64_t nodes, sols, steps;
     bool active;
 };
@@ -208,7 +220,7 @@ __device__ __forceinline__ uint32_t rec_t(const uint32_t* rec, uint32_t l)
 }
 
 __device__ __forceinline__ void load_record(const BtLaunch& P, ThreadItem& s, const uint32_t* rec, uint32_t* stk,
-                                            uint32_t* av, uint32_t* spill, uint32_t T, uint32_t tid)
+                                            uint64_t* av, uint64_t* spill, uint32_t T, uint32_t tid)
 {
     s.orig = static_cast<uint64_t>(rec[0]) | (static_cast<uint64_t>(rec[1]) << 32);
     const uint32_t len = rec[2] & 0xFFFFu;
@@ -218,18 +230,19 @@ __device__ __forceinline__ void load_record(const BtLaunch& P, ThreadItem& s, co
     s.tb = P.tables + P.puzzle_offset[s.pz];
     s.n = ldg(s.tb + H_N);
     s.ncol = ldg(s.tb + H_NCOL);
-    const uint32_t aw = ldg(s.tb + H_AWORDS);
-    const uint32_t init = ldg(s.tb + H_INIT);
-    for (uint32_t w = 0; w < aw; ++w) av[w * T + tid] = ldg(s.tb + init + w);
+    s.desc_off = ldg(s.tb + H_DESC);
+    const uint32_t aw = ldg(s.tb + H_AWORDS), init = ldg(s.tb + H_INIT);
+    for (uint32_t w = 0; w < aw; ++w) av[w * T + tid] = ldg64(s.tb + init + 2 * w);
     for (uint32_t l = 0; l < len; ++l) {
-        const LevelDesc d = load_desc(s.tb, l);
+        const LevelDesc d = load_desc(s.tb, s.desc_off, l);
         const uint32_t t = rec_t(rec, l);
-        av[(d.aoff + (t >> 5)) * T + tid] &= ~(0xFu << (t & 28u));
-        stk[l * T + tid] = (t << 21) | (ldg(s.tb + ldg(s.tb + H_TINFO + d.kind) + t) & 0xFFFFFu);
+        av[(d.aoff() + (t >> 6)) * T + tid] &= ~(0xFull << (t & 60u));
+        stk[l * T + tid] = (t << 21) | (ldg(s.tb + d.d5 + t) & 0xFFFFFu);
     }
     if (s.spilled) {
         const uint32_t* R = rec + P.rec_r_off;
-        for (uint32_t w = 0; w < P.max_kw; ++w) spill[len * P.max_kw + w] = R[w];
+        for (uint32_t w = 0; w < P.max_kw; ++w)
+            spill[len * P.max_kw + w] = static_cast<uint64_t>(R[2 * w]) | (static_cast<uint64_t>(R[2 * w + 1]) << 32);
     }
     s.L = len;
     s.base = len;
@@ -239,82 +252,98 @@ __device__ __forceinline__ void load_record(const BtLaunch& P, ThreadItem& s, co
     s.active = true;
 }
 
-// Candidates of the current level from bit `start` on, first non-empty word.
-struct Scan {
-    uint32_t w, x;
-};
-
-__device__ __forceinline__ Scan scan_level(const BtLaunch& P, const ThreadItem& s, const LevelDesc& d,
-                                           const uint32_t* const* sm, const uint32_t* stk, const uint32_t* av,
-                                           const uint32_t* sp, uint32_t start, bool spilled, uint32_t T,
-                                           uint32_t tid)
+// Candidate words of level L (not yet masked by the resume bit): the level's
+// pair-table row (frame sides & placed neighbours) & availability, or the
+// spilled remaining set.
+template <int KW>
+__device__ __forceinline__ void level_candidates(const BtLaunch& P, const ThreadItem& s, const LevelDesc& d,
+                                                 uint32_t L, bool spilled, const uint32_t* stk, const uint64_t* av,
+                                                 const uint64_t* spill, uint32_t T, uint32_t tid, uint64_t* x)
 {
-    Scan r{start >> 5, 0};
-    for (; r.w < d.kw; ++r.w) {
-        uint32_t x;
-        if (spilled) {
-            x = sp[r.w];
-        } else {
-            x = ldg(s.tb + d.base + r.w) & av[(d.aoff + r.w) * T + tid];
-            for (uint32_t j = 0; j < d.nplaced; ++j) x &= ldg(sm[j] + r.w);
-        }
-        if (r.w == (start >> 5)) x &= ~0u << (start & 31u);
-        if (x) {
-            r.x = x;
-            break;
+    const uint32_t kw = d.kw();
+    if (spilled) {
+        const uint64_t* sp = spill + L * P.max_kw;
+#pragma unroll
+        for (int w = 0; w < KW; ++w) x[w] = (uint32_t)w < kw ? sp[w] : 0ull;
+        return;
+    }
+    uint32_t row = d.d2;
+    if (d.arity() >= 1) {
+        const uint32_t ca = facing_colour(stk[d.level_a() * T + tid], d.side_a());
+        const uint32_t cb = d.arity() >= 2 ? facing_colour(stk[d.level_b() * T + tid], d.side_b()) : 0u;
+        row += ((d.arity() >= 2 ? ca * s.ncol + cb : ca) * kw) * 2;
+    }
+    const uint32_t* r = s.tb + row;
+#pragma unroll
+    for (int w = 0; w < KW; ++w) x[w] = (uint32_t)w < kw ? ldg64(r + 2 * w) & av[(d.aoff() + w) * T + tid] : 0ull;
+    if (d.nextra()) {
+        for (uint32_t j = 0; j < d.nextra(); ++j) {
+            const uint32_t sd = d.extra_side(j);
+            const uint32_t c = facing_colour(stk[d.extra_level(j) * T + tid], sd);
+            const uint32_t* sm = s.tb + d.d4 + ((sd * s.ncol + c) * kw) * 2;
+#pragma unroll
+            for (int w = 0; w < KW; ++w)
+                if ((uint32_t)w < kw) x[w] &= ldg64(sm + 2 * w);
         }
     }
-    return r;
 }
 
-__device__ __forceinline__ void side_masks(const ThreadItem& s, const LevelDesc& d, const uint32_t* stk, uint32_t T,
-                                           uint32_t tid, const uint32_t** sm)
+// First candidate at or after bit `start`; returns false when there is none.
+template <int KW>
+__device__ __forceinline__ bool first_candidate(const uint64_t* x, uint32_t start, uint32_t* t)
 {
-    for (uint32_t j = 0; j < d.nplaced; ++j) {
-        const uint32_t sd = desc_side(d, j);
-        const uint32_t c = (stk[desc_nb(d, j) * T + tid] >> (5 * ((sd + 2) & 3))) & 31u;
-        sm[j] = s.tb + ldg(s.tb + H_SIDE + d.kind) + (sd * s.ncol + c) * d.kw;
+    const uint32_t sw = start >> 6;
+    const uint64_t head = ~0ull << (start & 63u);
+    bool found = false;
+    uint32_t fw = 0;
+    uint64_t fx = 0;
+#pragma unroll
+    for (int w = 0; w < KW; ++w) {
+        uint64_t v = x[w];
+        v = (uint32_t)w < sw ? 0ull : ((uint32_t)w == sw ? v & head : v);
+        if (!found && v) {
+            found = true;
+            fw = w;
+            fx = v;
+        }
     }
+    *t = fw * 64 + __ffsll(fx) - 1;
+    return found;
 }
 
 // One step of emp_strategy::specific_run (include/emp_strategy.h:352-401)
 // inside the thread's record.  Returns false once the record is exhausted.
-__device__ __forceinline__ bool dfs_step(const BtLaunch& P, ThreadItem& s, uint32_t* stk, uint32_t* av,
-                                         uint32_t* spill, uint32_t T, uint32_t tid, bool* solved)
+template <int KW>
+__device__ __forceinline__ bool dfs_step(const BtLaunch& P, ThreadItem& s, uint32_t* stk, uint64_t* av,
+                                         uint64_t* spill, uint32_t T, uint32_t tid, bool* solved)
 {
-    const LevelDesc d = load_desc(s.tb, s.L);
-    const uint32_t* sm[4];
-    side_masks(s, d, stk, T, tid, sm);
-    uint32_t* sp = spill + s.L * P.max_kw;
-    const Scan c = scan_level(P, s, d, sm, stk, av, sp, s.start, s.spilled, T, tid);
-    if (c.w < d.kw) {
-        const uint32_t t = c.w * 32 + __ffs(c.x) - 1;
-        const uint32_t ti = ldg(s.tb + ldg(s.tb + H_TINFO + d.kind) + t);
+    const LevelDesc d = load_desc(s.tb, s.desc_off, s.L);
+    uint64_t x[KW];
+    level_candidates<KW>(P, s, d, s.L, s.spilled != 0, stk, av, spill, T, tid, x);
+    uint32_t t;
+    if (first_candidate<KW>(x, s.start, &t)) {
+        const uint32_t ti = ldg(s.tb + d.d5 + t);
+        const uint32_t kw = d.kw();
         if ((ti >> 20) & 1u) {
             // select_piece with an identical mask that clears other candidates
             // (emp_position_strategy.h:197-200): the level keeps its exact
             // remaining set from now on
-            const uint32_t* ex = s.tb + ldg(s.tb + H_EXTRA + d.kind) + t * d.kw;
-            for (uint32_t ww = 0; ww < d.kw; ++ww) {
-                uint32_t r;
-                if (s.spilled) {
-                    r = sp[ww];
-                } else {
-                    r = ldg(s.tb + d.base + ww) & av[(d.aoff + ww) * T + tid];
-                    for (uint32_t j = 0; j < d.nplaced; ++j) r &= ldg(sm[j] + ww);
-                }
-                sp[ww] = r & ldg(ex + ww);
-            }
+            if (!s.spilled) level_candidates<KW>(P, s, d, s.L, false, stk, av, spill, T, tid, x);
+            const uint32_t* ex = s.tb + d.d6 + t * kw * 2;
+            uint64_t* sp = spill + s.L * P.max_kw;
+#pragma unroll
+            for (int w = 0; w < KW; ++w)
+                if ((uint32_t)w < kw) sp[w] = x[w] & ldg64(ex + 2 * w);
             s.spilled = 1;
         }
-        av[(d.aoff + (t >> 5)) * T + tid] &= ~(0xFu << (t & 28u));
+        av[(d.aoff() + (t >> 6)) * T + tid] &= ~(0xFull << (t & 60u));
         stk[s.L * T + tid] = (t << 21) | (s.spilled << 20) | (ti & 0xFFFFFu);
         ++s.nodes;
         if (s.L == s.n - 1) {
             // solution: count it, give the piece back, try the next candidate
             ++s.sols;
             *solved = true;
-            av[(d.aoff + (t >> 5)) * T + tid] |= 0xFu << (t & 28u);
+            av[(d.aoff() + (t >> 6)) * T + tid] |= 0xFull << (t & 60u);
             s.start = t + 1;
         } else {
             ++s.L;
@@ -326,11 +355,11 @@ __device__ __forceinline__ bool dfs_step(const BtLaunch& P, ThreadItem& s, uint3
     if (s.L == s.base) return false;
     --s.L;
     const uint32_t e = stk[s.L * T + tid];
-    const uint32_t t = e >> 21;
+    const uint32_t tb = e >> 21;
     s.spilled = (e >> 20) & 1u;
-    const LevelDesc dl = load_desc(s.tb, s.L);
-    av[(dl.aoff + (t >> 5)) * T + tid] |= 0xFu << (t & 28u);
-    s.start = t + 1;
+    const LevelDesc dl = load_desc(s.tb, s.desc_off, s.L);
+    av[(dl.aoff() + (tb >> 6)) * T + tid] |= 0xFull << (tb & 60u);
+    s.start = tb + 1;
     return true;
 }
 
@@ -388,11 +417,12 @@ __device__ __forceinline__ void account(const BtLaunch& P, const ThreadItem& s)
 // Remaining candidates of level l (current level: from s.start; shallower
 // levels: after their placed transition), with `av` holding the availability
 // of level l's entry.
+template <int KW>
 __device__ __forceinline__ bool level_has_work(const BtLaunch& P, const ThreadItem& s, uint32_t l, const uint32_t* stk,
-                                               const uint32_t* av, const uint32_t* spill, uint32_t T, uint32_t tid,
+                                               const uint64_t* av, const uint64_t* spill, uint32_t T, uint32_t tid,
                                                uint32_t* start_out, uint32_t* spilled_out)
 {
-    const LevelDesc d = load_desc(s.tb, l);
+    const LevelDesc d = load_desc(s.tb, s.desc_off, l);
     uint32_t start, spilled;
     if (l == s.L) {
         start = s.start;
@@ -402,21 +432,21 @@ __device__ __forceinline__ bool level_has_work(const BtLaunch& P, const ThreadIt
         start = (e >> 21) + 1;
         spilled = (e >> 20) & 1u;
     }
-    const uint32_t* sm[4];
-    side_masks(s, d, stk, T, tid, sm);
-    const Scan c = scan_level(P, s, d, sm, stk, av, spill + l * P.max_kw, start, spilled != 0, T, tid);
+    uint64_t x[KW];
+    level_candidates<KW>(P, s, d, l, spilled != 0, stk, av, spill, T, tid, x);
+    uint32_t t;
     *start_out = start;
     *spilled_out = spilled;
-    return c.w < d.kw;
+    return first_candidate<KW>(x, start, &t);
 }
 
-__device__ __forceinline__ void toggle_piece(const ThreadItem& s, uint32_t l, const uint32_t* stk, uint32_t* av,
+__device__ __forceinline__ void toggle_piece(const ThreadItem& s, uint32_t l, const uint32_t* stk, uint64_t* av,
                                              uint32_t T, uint32_t tid, bool give_back)
 {
-    const LevelDesc d = load_desc(s.tb, l);
+    const LevelDesc d = load_desc(s.tb, s.desc_off, l);
     const uint32_t t = stk[l * T + tid] >> 21;
-    if (give_back) av[(d.aoff + (t >> 5)) * T + tid] |= 0xFu << (t & 28u);
-    else av[(d.aoff + (t >> 5)) * T + tid] &= ~(0xFu << (t & 28u));
+    if (give_back) av[(d.aoff() + (t >> 6)) * T + tid] |= 0xFull << (t & 60u);
+    else av[(d.aoff() + (t >> 6)) * T + tid] &= ~(0xFull << (t & 60u));
 }
 
 // Hands the remaining work of the thread's record to the next round: one
@@ -425,19 +455,20 @@ __device__ __forceinline__ void toggle_piece(const ThreadItem& s, uint32_t l, co
 // availability, and counts; pass 2 walks back down, writing records and taking
 // the pieces again, which leaves the state as it was.  Returns false when the
 // output queue is full (the thread then keeps the work).
-__device__ bool split_record(const BtLaunch& P, ThreadItem& s, uint32_t* stk, uint32_t* av, const uint32_t* spill,
+template <int KW>
+__device__ bool split_record(const BtLaunch& P, ThreadItem& s, uint32_t* stk, uint64_t* av, const uint64_t* spill,
                              uint32_t T, uint32_t tid)
 {
     uint32_t cnt = 0, start, spilled;
     for (uint32_t l = s.L + 1; l-- > s.base;) {
         if (l < s.L) toggle_piece(s, l, stk, av, T, tid, true);
-        cnt += level_has_work(P, s, l, stk, av, spill, T, tid, &start, &spilled);
+        cnt += level_has_work<KW>(P, s, l, stk, av, spill, T, tid, &start, &spilled);
     }
     const unsigned long long slot = cnt ? atomicAdd(P.out_tail, (unsigned long long)cnt) : 0ull;
     const bool fits = slot + cnt <= P.out_capacity;
     unsigned long long k = slot;
     for (uint32_t l = s.base; l <= s.L; ++l) {
-        if (level_has_work(P, s, l, stk, av, spill, T, tid, &start, &spilled)) {
+        if (level_has_work<KW>(P, s, l, stk, av, spill, T, tid, &start, &spilled)) {
             if (fits) {
                 uint32_t* rec = P.out_rec + k * P.rec_words;
                 rec[0] = static_cast<uint32_t>(s.orig);
@@ -450,7 +481,11 @@ __device__ bool split_record(const BtLaunch& P, ThreadItem& s, uint32_t* stk, ui
                     rec[4 + (j >> 1)] = lo | (hi << 16);
                 }
                 if (spilled)
-                    for (uint32_t w = 0; w < P.max_kw; ++w) rec[P.rec_r_off + w] = spill[l * P.max_kw + w];
+                    for (uint32_t w = 0; w < P.max_kw; ++w) {
+                        const uint64_t v = spill[l * P.max_kw + w];
+                        rec[P.rec_r_off + 2 * w] = static_cast<uint32_t>(v);
+                        rec[P.rec_r_off + 2 * w + 1] = static_cast<uint32_t>(v >> 32);
+                    }
             } else if (k < P.out_capacity) {
                 P.out_rec[k * P.rec_words + 3] = 1u << 17;  // reserved slot that fits: mark empty
             }
@@ -461,22 +496,24 @@ __device__ bool split_record(const BtLaunch& P, ThreadItem& s, uint32_t* stk, ui
     return fits;
 }
 
-template <int kStepsPerFetch>
+template <int KW, int kStepsPerFetch>
 __global__ void __launch_bounds__(256) dfs_kernel(BtLaunch P)
 {
-    extern __shared__ uint32_t smem[];
+    extern __shared__ __align__(16) uint32_t smem[];
     const uint32_t T = blockDim.x, tid = threadIdx.x, lane = tid & 31;
     uint32_t* stk = smem;
-    uint32_t* av = smem + P.max_levels * T;
-    uint32_t* spill = P.spill + (size_t)(blockIdx.x * T + tid) * P.max_levels * P.max_kw;
+    uint64_t* av = reinterpret_cast<uint64_t*>(smem + P.max_levels * T);
+    uint64_t* spill = P.spill + (size_t)(blockIdx.x * T + tid) * P.max_levels * P.max_kw;
     ThreadItem s;
     s.active = false;
     bool alive = true;
+    bool drained = false;      // warp-uniform: the input queue of this round is empty
+    uint32_t iteration = 0;    // warp-uniform loop counter
     uint32_t since_check = 0;  // steps since the last look at the global flags
     const uint64_t deadline = P.timeout_ns ? global_ns() + P.timeout_ns : 0;
     const uint32_t lt_mask = (1u << lane) - 1u;
 
-    for (;;) {
+    for (;; ++iteration) {
         // ---- work fetch: one atomic per warp, ranks from the ballot ----
         const bool need = alive && !s.active;
         const unsigned needmask = __ballot_sync(kFull, need);
@@ -485,6 +522,7 @@ __global__ void __launch_bounds__(256) dfs_kernel(BtLaunch P)
             unsigned long long base = 0;
             if (lane == leader) base = atomicAdd(P.cursor, (unsigned long long)__popc(needmask));
             base = __shfl_sync(kFull, base, leader);
+            if (base + __popc(needmask) >= P.n_in) drained = true;
             if (need) {
                 const uint64_t my = base + __popc(needmask & lt_mask);
                 if (my < P.n_in && !*(volatile int*)P.abort_flag) {
@@ -498,13 +536,19 @@ __global__ void __launch_bounds__(256) dfs_kernel(BtLaunch P)
                     alive = false;
                 }
             }
+        } else if (!drained && (iteration & 31u) == 31u) {
+            // every warp learns within 32 rounds of steps that the queue ran dry
+            unsigned long long c = 0;
+            if (lane == 0) c = *(volatile unsigned long long*)P.cursor;
+            c = __shfl_sync(kFull, c, 0);
+            drained = c >= P.n_in;
         }
         if (!__any_sync(kFull, alive)) break;
 
         // ---- DFS steps ----
         for (int step = 0; step < kStepsPerFetch && s.active; ++step) {
             bool solved = false;
-            if (dfs_step(P, s, stk, av, spill, T, tid, &solved)) {
+            if (dfs_step<KW>(P, s, stk, av, spill, T, tid, &solved)) {
                 if (solved) record_solution(P, s, stk, T, tid);
                 continue;
             }
@@ -515,11 +559,12 @@ __global__ void __launch_bounds__(256) dfs_kernel(BtLaunch P)
         s.steps += kStepsPerFetch;
         since_check += kStepsPerFetch;
 
-        // ---- hand work back once over budget ----
-        if (P.item_budget && s.steps >= P.item_budget) {
-            if (split_record(P, s, stk, av, spill, T, tid)) {
+        // ---- once the queue is empty, hand work back for the next round ----
+        if (drained && P.item_budget && s.steps >= P.item_budget) {
+            if (split_record<KW>(P, s, stk, av, spill, T, tid)) {
                 account(P, s);
                 s.active = false;
+                alive = false;
                 continue;
             }
             s.steps = 0;
@@ -592,6 +637,24 @@ __global__ void record_prefix(const uint32_t* __restrict__ rec, uint32_t rec_wor
     for (uint32_t l = threadIdx.x; l < len; l += blockDim.x) out[l] = static_cast<uint16_t>(rec_t(r, l));
 }
 
+template <int KW>
+const void* dfs_symbol() { return reinterpret_cast<const void*>(&dfs_kernel<KW, 32>); }
+
+const void* dfs_symbol_for(uint32_t max_kw)
+{
+    switch (max_kw) {
+        case 1: return dfs_symbol<1>();
+        case 2: return dfs_symbol<2>();
+        case 3: return dfs_symbol<3>();
+        case 4: return dfs_symbol<4>();
+        case 5: return dfs_symbol<5>();
+        case 6: return dfs_symbol<6>();
+        case 7: return dfs_symbol<7>();
+        case 8: return dfs_symbol<8>();
+        default: return max_kw <= 16 ? dfs_symbol<16>() : nullptr;
+    }
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -626,16 +689,20 @@ uint64_t scan_block_sum_words(uint64_t n) { return (n + kScanBlock - 1) / kScanB
 
 size_t dfs_smem_bytes(uint32_t max_levels, uint32_t max_avail_words, uint32_t threads)
 {
-    return static_cast<size_t>(max_levels + max_avail_words) * threads * sizeof(uint32_t);
+    return (static_cast<size_t>(max_levels) * sizeof(uint32_t) + static_cast<size_t>(max_avail_words) * 8) * threads;
 }
 
-uint32_t record_words(uint32_t max_levels, uint32_t max_kw) { return 4 + (max_levels + 1) / 2 + max_kw; }
+uint32_t record_words(uint32_t max_levels, uint32_t max_kw) { return 4 + (max_levels + 1) / 2 + 2 * max_kw; }
+
+const void* dfs_kernel_symbol(uint32_t max_kw) { return dfs_symbol_for(max_kw); }
 
 cudaError_t launch_dfs(const BtLaunch& P, uint32_t blocks, uint32_t threads, cudaStream_t stream)
 {
+    const void* fn = dfs_symbol_for(P.max_kw);
+    if (!fn) return cudaErrorInvalidValue;
     const size_t smem = dfs_smem_bytes(P.max_levels, P.max_avail_words, threads);
-    dfs_kernel<32><<<blocks, threads, smem, stream>>>(P);
-    return cudaGetLastError();
+    void* args[] = {const_cast<BtLaunch*>(&P)};
+    return cudaLaunchKernel(fn, dim3(blocks), dim3(threads), args, smem, stream);
 }
 
 cudaError_t launch_bt_reset(const BtLaunch& P, uint32_t n_puzzles, cudaStream_t stream)
@@ -661,7 +728,5 @@ cudaError_t launch_record_prefix(const uint32_t* rec, uint32_t rec_words, uint64
     record_prefix<<<1, 64, 0, stream>>>(rec, rec_words, i, out);
     return cudaGetLastError();
 }
-
-const void* dfs_kernel_symbol() { return reinterpret_cast<const void*>(&dfs_kernel<32>); }
 
 }  // namespace emp

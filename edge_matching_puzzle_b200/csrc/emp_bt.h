@@ -29,9 +29,9 @@ struct BtLaunch {
     const uint64_t* puzzle_offset = nullptr;  // word offset of each puzzle blob
     uint32_t depth = 0;                       // split depth (prefix expansion)
     uint32_t max_levels = 0;                  // max pieces over the puzzles of the launch
-    uint32_t max_avail_words = 0;             // max availability words (three kinds)
-    uint32_t max_kw = 0;                      // max words of one kind
-    uint32_t* spill = nullptr;                // [threads][max_levels][max_kw] remaining sets
+    uint32_t max_avail_words = 0;             // max 64-bit availability words (three kinds)
+    uint32_t max_kw = 0;                      // max 64-bit words of one kind
+    uint64_t* spill = nullptr;                // [threads][max_levels][max_kw] remaining sets
     // work records of this round and of the next one
     const uint32_t* in_rec = nullptr;
     uint64_t n_in = 0;
@@ -69,6 +69,6 @@ cudaError_t launch_make_records(const uint16_t* prefixes, const uint32_t* prefix
                                 cudaStream_t stream);
 cudaError_t launch_record_prefix(const uint32_t* rec, uint32_t rec_words, uint64_t i, uint16_t* out,
                                  cudaStream_t stream);
-const void* dfs_kernel_symbol();
+const void* dfs_kernel_symbol(uint32_t max_kw);
 
 }  // namespace emp

@@ -1,4 +1,4 @@
-// Device side of the exhaustive backtracker (sm_100a).
+// Device-side table access of the exhaustive backtracker (sm_100a).
 //
 // The search is the reference's emp_strategy::specific_run
 // (include/emp_strategy.h:343-410): a depth-first walk over the levels of a
@@ -9,7 +9,8 @@
 // at the last level is a solution.  With identical pieces, trying t also
 // removes the bits of its identical mask (:189-202).
 //
-// Table blob layout: see emp_model.h (DeviceTables, header words 0..31).
+// Table blob layout: emp_model.h (DeviceTables).  Candidate bit t =
+// kind_index*4 + orientation lives in 64-bit word t>>6, bit t&63.
 #pragma once
 
 #include <cstdint>
@@ -19,34 +20,42 @@ namespace dev {
 
 // header word indices of a puzzle blob
 enum : uint32_t {
-    H_N = 1, H_NCOL = 2, H_KW = 3, H_AOFF = 6, H_AWORDS = 9, H_SIDE = 10, H_BASE = 13,
-    H_DESC = 14, H_TINFO = 15, H_EXTRA = 18, H_INIT = 21, H_W = 22, H_H = 23, H_SIZE = 24,
-    H_DEPTH = 25
+    H_N = 1, H_NCOL = 2, H_KW = 3, H_AOFF = 6, H_AWORDS = 9, H_SIDE = 10, H_PAIR = 13, H_DESC = 14, H_TINFO = 15,
+    H_EXTRA = 18, H_INIT = 21, H_W = 22, H_H = 23, H_SIZE = 24, H_MAXKW = 25
 };
 
 __device__ __forceinline__ uint32_t ldg(const uint32_t* p) { return __ldg(p); }
-
-// level descriptor fields (emp_model.cpp build_device_tables)
-struct LevelDesc {
-    uint32_t kind, nplaced, kw, aoff, base, w0, w1;
-};
-
-__device__ __forceinline__ LevelDesc load_desc(const uint32_t* tb, uint32_t L)
+__device__ __forceinline__ uint64_t ldg64(const uint32_t* p)
 {
-    const uint32_t* d = tb + ldg(tb + H_DESC) + 4 * L;
-    LevelDesc r;
-    r.w0 = ldg(d);
-    r.w1 = ldg(d + 1);
-    r.base = ldg(d + 2);
-    r.aoff = ldg(d + 3) & 0xFFFFu;
-    r.kind = r.w0 & 3u;
-    r.nplaced = (r.w0 >> 2) & 7u;
-    r.kw = (r.w0 >> 16) & 0xFFu;
-    return r;
+    return __ldg(reinterpret_cast<const unsigned long long*>(p));
 }
 
-__device__ __forceinline__ uint32_t desc_side(const LevelDesc& d, uint32_t j) { return (d.w0 >> (5 + 2 * j)) & 3u; }
-__device__ __forceinline__ uint32_t desc_nb(const LevelDesc& d, uint32_t j) { return (d.w1 >> (8 * j)) & 0xFFu; }
+struct LevelDesc {
+    uint32_t d0, d1, d2, d3, d4, d5, d6, d7;
+    __device__ __forceinline__ uint32_t kind() const { return d0 & 3u; }
+    __device__ __forceinline__ uint32_t nplaced() const { return (d0 >> 2) & 7u; }
+    __device__ __forceinline__ uint32_t kw() const { return (d0 >> 8) & 0xFFu; }
+    __device__ __forceinline__ uint32_t aoff() const { return d0 >> 16; }
+    __device__ __forceinline__ uint32_t arity() const { return d1 & 3u; }
+    __device__ __forceinline__ uint32_t side_a() const { return (d1 >> 2) & 3u; }
+    __device__ __forceinline__ uint32_t side_b() const { return (d1 >> 4) & 3u; }
+    __device__ __forceinline__ uint32_t level_a() const { return (d1 >> 8) & 0xFFu; }
+    __device__ __forceinline__ uint32_t level_b() const { return (d1 >> 16) & 0xFFu; }
+    __device__ __forceinline__ uint32_t nextra() const { return (d1 >> 24) & 3u; }
+    __device__ __forceinline__ uint32_t extra_side(uint32_t j) const { return (d3 >> (2 * j)) & 3u; }
+    __device__ __forceinline__ uint32_t extra_level(uint32_t j) const { return (d3 >> (8 + 8 * j)) & 0xFFu; }
+};
+
+__device__ __forceinline__ LevelDesc load_desc(const uint32_t* tb, uint32_t desc_off, uint32_t L)
+{
+    const uint4* d = reinterpret_cast<const uint4*>(tb + desc_off + 8 * L);
+    const uint4 a = __ldg(d), b = __ldg(d + 1);
+    return LevelDesc{a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+}
+
+// colour that the neighbour placed at the level whose stack word is `e`
+// shows towards my side `s` (its side (s+2)&3); 5 bits per side
+__device__ __forceinline__ uint32_t facing_colour(uint32_t e, uint32_t s) { return (e >> (5 * ((s + 2) & 3u))) & 31u; }
 
 }  // namespace dev
 }  // namespace emp

@@ -218,116 +218,192 @@ bool build_plan(const PuzzleModel& m, const std::vector<uint32_t>& order,
     return true;
 }
 
+namespace {
+
+inline void set_bit64(uint64_t* w, uint32_t i) { w[i >> 6] |= uint64_t(1) << (i & 63); }
+
+void push64(std::vector<uint32_t>& b, uint64_t v)
+{
+    b.push_back(static_cast<uint32_t>(v));
+    b.push_back(static_cast<uint32_t>(v >> 32));
+}
+
+void align(std::vector<uint32_t>& b, size_t words)
+{
+    while (b.size() % words) b.push_back(0);
+}
+
+}  // namespace
+
 void build_device_tables(const PuzzleModel& m, const std::vector<LevelPlan>& plan, DeviceTables& t)
 {
     t = DeviceTables();
     t.n = m.n;
     t.ncol = m.border_id + 1;
-    uint32_t off = kHeaderWords;
     for (uint32_t k = 0; k < 3; ++k) {
-        t.kw[k] = m.kind_words[k];
-        t.avail_off[k] = t.avail_words;
+        t.kw[k] = (4 * m.nb_kind(k) + 63) / 64;
+        t.aoff[k] = t.avail_words;
         t.avail_words += t.kw[k];
+        t.max_kw = std::max(t.max_kw, t.kw[k]);
     }
     std::vector<uint32_t>& b = t.blob;
     b.assign(kHeaderWords, 0);
-    // side masks [k][s][c][kw]: bit (ki,o) when side s of piece ki@o shows colour
-    // c (c = border_id for a frame side), for allowed orientations only
-    t.side_off = off;
+    // side masks per kind: bit (ki,o) when side s of piece ki@o shows colour c
+    // (c = border_id for a frame side), for allowed orientations only
+    std::array<std::vector<uint64_t>, 3> side;
     for (uint32_t k = 0; k < 3; ++k) {
-        t.side_kind_off[k] = static_cast<uint32_t>(b.size());
-        b.resize(b.size() + static_cast<size_t>(4) * t.ncol * t.kw[k], 0);
+        side[k].assign(static_cast<size_t>(4) * t.ncol * t.kw[k], 0);
         for (uint32_t ki = 0; ki < m.nb_kind(k); ++ki) {
-            uint32_t p = m.members[k][ki];
+            const uint32_t p = m.members[k][ki];
             for (uint32_t o = 0; o < 4; ++o) {
                 if (!m.allowed(p, o)) continue;
                 for (uint32_t s = 0; s < 4; ++s) {
                     uint32_t c = m.colour(p, s, o);
                     if (!c) c = m.border_id;
-                    uint32_t* w = &b[t.side_kind_off[k] + (static_cast<size_t>(s) * t.ncol + c) * t.kw[k]];
-                    set_bit(w, 4 * ki + o);
+                    set_bit64(&side[k][(static_cast<size_t>(s) * t.ncol + c) * t.kw[k]], 4 * ki + o);
                 }
             }
         }
+        align(b, 4);
+        t.side_off[k] = static_cast<uint32_t>(b.size());
+        for (uint64_t v : side[k]) push64(b, v);
     }
-    // per level descriptors and base masks
-    t.desc_off = static_cast<uint32_t>(b.size());
-    b.resize(b.size() + 4 * static_cast<size_t>(m.n), 0);
-    t.base_off = static_cast<uint32_t>(b.size());
+    // pair tables, one per distinct (kind, base, paired sides) class
+    align(b, 4);
+    t.pair_off = static_cast<uint32_t>(b.size());
+    struct Key {
+        uint32_t kind, arity, sa, sb;
+        std::vector<uint32_t> base;
+        bool operator==(const Key& o) const
+        {
+            return kind == o.kind && arity == o.arity && sa == o.sa && sb == o.sb && base == o.base;
+        }
+    };
+    std::vector<std::pair<Key, uint32_t>> classes;
+    std::vector<uint32_t> level_pair(m.n);
     for (uint32_t L = 0; L < m.n; ++L) {
         const LevelPlan& lp = plan[L];
-        uint32_t boff = static_cast<uint32_t>(b.size());
-        b.insert(b.end(), lp.base.begin(), lp.base.end());
-        uint32_t w0 = lp.kind | (lp.nplaced << 2);
-        uint32_t w1 = 0;
-        for (uint32_t j = 0; j < lp.nplaced; ++j) {
-            w0 |= static_cast<uint32_t>(lp.side[j]) << (5 + 2 * j);
-            w1 |= static_cast<uint32_t>(lp.nb_level[j]) << (8 * j);
+        Key key{lp.kind, std::min<uint32_t>(lp.nplaced, 2), lp.nplaced > 0 ? lp.side[0] : 0u,
+                lp.nplaced > 1 ? lp.side[1] : 0u, lp.base};
+        uint32_t off = 0;
+        bool found = false;
+        for (const auto& c : classes)
+            if (c.first == key) {
+                off = c.second;
+                found = true;
+                break;
+            }
+        if (!found) {
+            align(b, 4);
+            off = static_cast<uint32_t>(b.size());
+            const uint32_t k = key.kind, kw = t.kw[k];
+            std::vector<uint64_t> base64(kw, 0);
+            for (uint32_t i = 0; i < 4 * m.nb_kind(k); ++i)
+                if ((lp.base[i >> 5] >> (i & 31)) & 1u) set_bit64(base64.data(), i);
+            const uint32_t na = key.arity >= 1 ? t.ncol : 1, nb = key.arity >= 2 ? t.ncol : 1;
+            for (uint32_t ca = 0; ca < na; ++ca)
+                for (uint32_t cb = 0; cb < nb; ++cb)
+                    for (uint32_t w = 0; w < kw; ++w) {
+                        uint64_t v = base64[w];
+                        if (key.arity >= 1) v &= side[k][(static_cast<size_t>(key.sa) * t.ncol + ca) * kw + w];
+                        if (key.arity >= 2) v &= side[k][(static_cast<size_t>(key.sb) * t.ncol + cb) * kw + w];
+                        push64(b, v);
+                    }
+            classes.push_back({key, off});
         }
-        w0 |= t.kw[lp.kind] << 16;
-        b[t.desc_off + 4 * L + 0] = w0;
-        b[t.desc_off + 4 * L + 1] = w1;
-        b[t.desc_off + 4 * L + 2] = boff;
-        b[t.desc_off + 4 * L + 3] = t.avail_off[lp.kind] | (lp.position << 16);
+        level_pair[L] = off;
     }
-    // transition info: colours of piece@o (5 bits per side) and the has-extra flag
-    t.tinfo_off = static_cast<uint32_t>(b.size());
+    // level descriptors
+    align(b, 4);
+    t.desc_off = static_cast<uint32_t>(b.size());
+    b.resize(b.size() + 8 * static_cast<size_t>(m.n), 0);
+    // transition info
     for (uint32_t k = 0; k < 3; ++k) {
-        t.tinfo_kind_off[k] = static_cast<uint32_t>(b.size());
-        uint32_t bits = 4 * m.nb_kind(k);
+        align(b, 2);
+        t.tinfo_off[k] = static_cast<uint32_t>(b.size());
+        const uint32_t bits = 4 * m.nb_kind(k);
         for (uint32_t e = 0; e < bits; ++e) {
-            uint32_t p = m.members[k][e >> 2], o = e & 3, v = 0;
+            const uint32_t p = m.members[k][e >> 2], o = e & 3;
+            uint32_t v = 0;
             for (uint32_t s = 0; s < 4; ++s) v |= m.colour(p, s, o) << (5 * s);
             // extra clears: bits the identical mask removes besides e itself,
             // restricted to allowed candidates (others never appear in a set)
-            bool extra = false;
-            const uint32_t* im = &m.idmask[k][static_cast<size_t>(e) * t.kw[k]];
-            for (uint32_t e2 = 0; e2 < bits && !extra; ++e2) {
-                if (e2 == e) continue;
-                if (!m.allowed(m.members[k][e2 >> 2], e2 & 3)) continue;
-                if (!((im[e2 >> 5] >> (e2 & 31)) & 1)) extra = true;
+            const uint32_t* im = &m.idmask[k][static_cast<size_t>(e) * m.kind_words[k]];
+            for (uint32_t e2 = 0; e2 < bits; ++e2) {
+                if (e2 == e || !m.allowed(m.members[k][e2 >> 2], e2 & 3)) continue;
+                if (!((im[e2 >> 5] >> (e2 & 31)) & 1u)) {
+                    v |= 1u << 20;
+                    break;
+                }
             }
-            if (extra) v |= 1u << 20;
             b.push_back(v);
         }
     }
-    t.extra_off = static_cast<uint32_t>(b.size());
     for (uint32_t k = 0; k < 3; ++k) {
-        t.extra_kind_off[k] = static_cast<uint32_t>(b.size());
-        uint32_t bits = 4 * m.nb_kind(k);
+        align(b, 2);
+        t.extra_off[k] = static_cast<uint32_t>(b.size());
+        const uint32_t bits = 4 * m.nb_kind(k);
         for (uint32_t e = 0; e < bits; ++e) {
-            const uint32_t* im = &m.idmask[k][static_cast<size_t>(e) * t.kw[k]];
-            for (uint32_t w = 0; w < t.kw[k]; ++w) b.push_back(im[w]);
+            const uint32_t* im = &m.idmask[k][static_cast<size_t>(e) * m.kind_words[k]];
+            for (uint32_t w = 0; w < t.kw[k]; ++w) {
+                uint64_t v = 0;
+                for (uint32_t i = 0; i < 64; ++i) {
+                    const uint32_t bit = 64 * w + i;
+                    // bits past the kind's candidates stay 1, like the reference's all-ones init
+                    const bool one = bit >= bits || ((im[bit >> 5] >> (bit & 31)) & 1u);
+                    if (one) v |= uint64_t(1) << i;
+                }
+                push64(b, v);
+            }
         }
     }
-    t.init_avail_off = static_cast<uint32_t>(b.size());
+    align(b, 2);
+    t.init_off = static_cast<uint32_t>(b.size());
     for (uint32_t k = 0; k < 3; ++k) {
-        uint32_t bits = 4 * m.nb_kind(k);
+        const uint32_t bits = 4 * m.nb_kind(k);
         for (uint32_t w = 0; w < t.kw[k]; ++w) {
-            uint32_t v = 0;
-            for (uint32_t i = 0; i < 32; ++i)
-                if (w * 32 + i < bits) v |= 1u << i;
-            b.push_back(v);
+            uint64_t v = 0;
+            for (uint32_t i = 0; i < 64; ++i)
+                if (w * 64 + i < bits) v |= uint64_t(1) << i;
+            push64(b, v);
         }
     }
-    // header
-    b[0] = 0x454D5031u;  // "EMP1"
+    align(b, 4);
+    for (uint32_t L = 0; L < m.n; ++L) {
+        const LevelPlan& lp = plan[L];
+        uint32_t* d = &b[t.desc_off + 8 * L];
+        const uint32_t k = lp.kind;
+        d[0] = k | (lp.nplaced << 2) | (t.kw[k] << 8) | (t.aoff[k] << 16);
+        const uint32_t arity = std::min<uint32_t>(lp.nplaced, 2);
+        d[1] = arity | ((arity > 0 ? lp.side[0] : 0u) << 2) | ((arity > 1 ? lp.side[1] : 0u) << 4) |
+               ((arity > 0 ? lp.nb_level[0] : 0u) << 8) | ((arity > 1 ? lp.nb_level[1] : 0u) << 16) |
+               ((lp.nplaced - arity) << 24);
+        d[2] = level_pair[L];
+        d[3] = (lp.nplaced > 2 ? lp.side[2] : 0u) | ((lp.nplaced > 3 ? lp.side[3] : 0u) << 2) |
+               ((lp.nplaced > 2 ? lp.nb_level[2] : 0u) << 8) | ((lp.nplaced > 3 ? lp.nb_level[3] : 0u) << 16);
+        d[4] = t.side_off[k];
+        d[5] = t.tinfo_off[k];
+        d[6] = t.extra_off[k];
+        d[7] = lp.position;
+    }
+    b[0] = 0x454D5032u;  // "EMP2"
     b[1] = t.n;
     b[2] = t.ncol;
     for (uint32_t k = 0; k < 3; ++k) {
         b[3 + k] = t.kw[k];
-        b[6 + k] = t.avail_off[k];
-        b[10 + k] = t.side_kind_off[k];
-        b[15 + k] = t.tinfo_kind_off[k];
-        b[18 + k] = t.extra_kind_off[k];
+        b[6 + k] = t.aoff[k];
+        b[10 + k] = t.side_off[k];
+        b[15 + k] = t.tinfo_off[k];
+        b[18 + k] = t.extra_off[k];
     }
     b[9] = t.avail_words;
-    b[13] = t.base_off;
+    b[13] = t.pair_off;
     b[14] = t.desc_off;
-    b[21] = t.init_avail_off;
+    b[21] = t.init_off;
     b[22] = m.width;
     b[23] = m.height;
     b[24] = static_cast<uint32_t>(b.size());
+    b[25] = t.max_kw;
 }
 
 namespace {

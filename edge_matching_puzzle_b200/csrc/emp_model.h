@@ -74,24 +74,35 @@ struct LevelPlan {
     std::vector<uint32_t> base;        // frame-side masks & allowed orientations
 };
 
-// Flattened tables consumed by the GPU kernels (one blob per puzzle).
-// Offsets are in 32-bit words from the start of the blob.
+// Flattened tables consumed by the GPU kernels (one blob per puzzle), 32-bit
+// words; every 64-bit table starts on an even word and the blob size is a
+// multiple of 4 words so blobs can be concatenated keeping 16-byte alignment.
+//
+// header (kHeaderWords words):
+//   0 magic, 1 n, 2 ncol (= border_id + 1), 3..5 kw[k] (64-bit words per kind),
+//   6..8 aoff[k] (64-bit word offset of kind k in the availability array),
+//   9 avail words (64-bit), 10..12 side[k], 13 pair section, 14 desc,
+//   15..17 tinfo[k], 18..20 extra[k], 21 initial availability, 22 width,
+//   23 height, 24 blob words, 25 max kw
+// desc (8 words per level):
+//   d0 kind | nplaced<<2 | kw<<8 | aoff<<16
+//   d1 pair arity | sideA<<2 | sideB<<4 | levelA<<8 | levelB<<16 | nextra<<24
+//   d2 pair table (word offset): arity 2 [cA][cB][kw], 1 [cA][kw], 0 [kw];
+//      entries = frame-side masks & allowed orientations & placed-side masks
+//   d3 extra placed sides: side3 | side4<<2 | level3<<8 | level4<<16
+//   d4 side[kind], d5 tinfo[kind], d6 extra[kind], d7 position
+// side[k]: 64-bit [side][colour][kw[k]] masks (colour ncol-1 = frame)
+// tinfo[k]: per transition t, colours of the oriented piece (5 bits per side)
+//           | has_extra<<20 (its identical mask clears other candidates)
+// extra[k]: 64-bit [4*nk][kw[k]] identical masks
 struct DeviceTables {
     std::vector<uint32_t> blob;
-    uint32_t n = 0, ncol = 0;           // ncol = border_id + 1
-    std::array<uint32_t, 3> kw{};       // words per kind
-    std::array<uint32_t, 3> avail_off{};// offset of each kind in the per-thread availability
-    uint32_t avail_words = 0;
-    uint32_t side_off = 0;   // [k][s][c][kw[k]] with kind base offsets side_kind_off
-    std::array<uint32_t, 3> side_kind_off{};
-    uint32_t base_off = 0;   // per level: base_level_off[L]
-    uint32_t desc_off = 0;   // per level: 2 words
-    uint32_t tinfo_off = 0;  // [k][4nk]: colours (5 bits x 4) | has_extra << 20
-    std::array<uint32_t, 3> tinfo_kind_off{};
-    uint32_t extra_off = 0;  // [k][4nk][kw] extra identical clears (all ones = none)
-    std::array<uint32_t, 3> extra_kind_off{};
-    uint32_t init_avail_off = 0;
-    uint32_t tcount_off = 0; // transitions per kind
+    uint32_t n = 0, ncol = 0, max_kw = 0;
+    std::array<uint32_t, 3> kw{};       // 64-bit words per kind
+    std::array<uint32_t, 3> aoff{};     // availability offset of each kind (64-bit words)
+    uint32_t avail_words = 0;           // 64-bit words
+    std::array<uint32_t, 3> side_off{}, tinfo_off{}, extra_off{};
+    uint32_t desc_off = 0, pair_off = 0, init_off = 0;
 };
 
 bool build_plan(const PuzzleModel& m, const std::vector<uint32_t>& order,

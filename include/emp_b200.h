@@ -105,8 +105,9 @@ typedef struct emp_bt_config {
     uint32_t timeout_ms;         /* kernel deadline; 0 = none */
     int32_t device;              /* CUDA device ordinal; -1 = current device */
     uint32_t keep_subtree_counts;/* 1: keep per-subtree counts for emp_bt_plan_subtree_counts */
-    uint32_t split_budget;       /* DFS steps a thread spends on a work record before handing the
-                                    rest back as new records; 0 = default (32768) */
+    uint32_t split_budget;       /* once a round's queue is empty, a thread that spent this many
+                                    DFS steps on its work record hands the rest back as new records
+                                    for the next round; 0 = default (2048) */
     uint32_t reserved[6];
 } emp_bt_config;
 

@@ -68,20 +68,31 @@ def test_invalid_puzzles_rejected():
 
 def _decode(blob):
     hdr = blob[:32]
-    return dict(n=hdr[1], ncol=hdr[2], kw=hdr[3:6], aoff=hdr[6:9], aw=hdr[9], side=hdr[10:13], base=hdr[13],
+    return dict(n=hdr[1], ncol=hdr[2], kw=hdr[3:6], aoff=hdr[6:9], aw=hdr[9], side=hdr[10:13], pair=hdr[13],
                 desc=hdr[14], tinfo=hdr[15:18], extra=hdr[18:21], init=hdr[21], w=hdr[22], h=hdr[23])
 
 
+def _u64(blob, off, count):
+    return [blob[off + 2 * i] | (blob[off + 2 * i + 1] << 32) for i in range(count)]
+
+
 def _candidates_from_tables(blob, h, level, neighbour_colours):
-    d = blob[h["desc"] + 4 * level: h["desc"] + 4 * level + 4]
-    kind, nplaced, kw = d[0] & 3, (d[0] >> 2) & 7, (d[0] >> 16) & 0xFF
-    words = list(blob[d[2]: d[2] + kw])
-    for j in range(nplaced):
-        side = (d[0] >> (5 + 2 * j)) & 3
-        c = neighbour_colours[side]
-        off = h["side"][kind] + (side * h["ncol"] + c) * kw
-        words = [a & b for a, b in zip(words, blob[off: off + kw])]
-    return kind, sum(w << (32 * i) for i, w in enumerate(words)), [(d[0] >> (5 + 2 * j)) & 3 for j in range(nplaced)]
+    """Decodes a level descriptor and returns (kind, candidate bits, placed sides):
+    pair-table row for the first two placed sides & side masks of the others."""
+    d = blob[h["desc"] + 8 * level: h["desc"] + 8 * level + 8]
+    kind, nplaced, kw = d[0] & 3, (d[0] >> 2) & 7, (d[0] >> 8) & 0xFF
+    arity = d[1] & 3
+    sides = [(d[1] >> 2) & 3, (d[1] >> 4) & 3][:arity] + [(d[3] >> (2 * j)) & 3 for j in range(nplaced - arity)]
+    row = d[2]
+    if arity == 1:
+        row += neighbour_colours[sides[0]] * kw * 2
+    elif arity == 2:
+        row += (neighbour_colours[sides[0]] * h["ncol"] + neighbour_colours[sides[1]]) * kw * 2
+    words = _u64(blob, row, kw)
+    for sd in sides[arity:]:
+        off = d[4] + (sd * h["ncol"] + neighbour_colours[sd]) * kw * 2
+        words = [a & b for a, b in zip(words, _u64(blob, off, kw))]
+    return kind, sum(w << (64 * i) for i, w in enumerate(words)), sides
 
 
 @pytest.mark.parametrize("seed", [0, 1, 2, 3])
@@ -133,9 +144,9 @@ def test_identical_masks_match_oracle(seed):
     assert bool(npz.info().has_identical) == op.has_identical
     for kind in range(3):
         kw = hd["kw"][kind]
-        for t in range(4 * op.nb_kind(kind)):
+        bits = 4 * op.nb_kind(kind)
+        for t in range(bits):
             m64 = op.identical_mask(kind, t)
-            m = sum(v << (64 * i) for i, v in enumerate(m64)) & ((1 << (32 * kw)) - 1)
-            off = hd["extra"][kind] + t * kw
-            got = sum(v << (32 * i) for i, v in enumerate(blob[off: off + kw]))
-            assert got == m
+            m = sum(v << (64 * i) for i, v in enumerate(m64)) & ((1 << bits) - 1)
+            got = sum(v << (64 * i) for i, v in enumerate(_u64(blob, hd["extra"][kind] + t * kw * 2, kw)))
+            assert got & ((1 << bits) - 1) == m
