@@ -1,0 +1,392 @@
+#!/usr/bin/env python
+"""Benchmark of the exhaustive backtracker: placements/s on B200.
+
+Workload: the project's 8x8 exhaustive count (4 border / 8 interior colours, seeds
+0..15, generated by emp_generate_puzzle, row-major "basic" order, split depth 12).  The
+whole count is about 5e12 placements, so one step processes one slice of it: the
+depth-12 subtrees s, s+64, s+128, ... of all 16 puzzles (a different slice per step,
+64 slices make the complete count).  A placement is one node of the reference's
+emp_strategy search (include/emp_strategy.h:358).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line (rank 0).  value: placements/s with the puzzle tables and the
+depth-12 prefixes resident on the device; e2e: the same metric through the one-shot
+public call emp_bt_count_batch with host-side inputs (table upload, prefix expansion,
+all rounds, result download inside the timed region).  The reference arm times the CPU
+restatement of emp_strategy (oracle/, the reference itself cannot be built here: its
+sibling libraries are not available) on all host cores over a bounded sample of the
+same subtrees.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WIDTH, HEIGHT, BORDER, INTERIOR = 8, 8, 4, 8
+SEEDS = list(range(16))
+DEPTH = 12
+SLICES = 64
+CPU_STRIDE = 4096
+METRIC = "placements/s on 1 B200; time-to-first-solution, learned vs plain ordering"
+UNIT = "placements/s"
+WORKLOAD = (f"exhaustive row-major count of 16 seeded {WIDTH}x{HEIGHT} puzzles ({BORDER} border / {INTERIOR} interior "
+            f"colours, seeds 0..15), split depth {DEPTH}, one step = 1/{SLICES} slice of the depth-{DEPTH} subtrees")
+L2_BYTES = 126 * 1024 * 1024
+
+
+def env_int(name, default):
+    try:
+        return int(os.environ.get(name, default))
+    except ValueError:
+        return default
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return d, "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "sm_max_mhz": 1965.0}, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.file = None
+
+    def __enter__(self):
+        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.file,
+                                         stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.file:
+            return None
+        self.file.flush()
+        with open(self.file.name) as f:
+            rows = [r.strip().split(", ") for r in f if r.strip()]
+        os.unlink(self.file.name)
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx = max(mx, float(r[2]))
+                for n, v in zip(names, r[5:9]):
+                    if v.strip().lower() == "active":
+                        reasons.add(n)
+            except (ValueError, IndexError):
+                continue
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def make_puzzles():
+    from edge_matching_puzzle_b200 import native
+    return [native.NativePuzzle(WIDTH, HEIGHT, native.generate(WIDTH, HEIGHT, BORDER, INTERIOR, s)) for s in SEEDS]
+
+
+def algorithmic_work(kind_nodes, puzzle):
+    """Per-placement work of the search (32-bit words W_k of the placed kind's
+    bitfield): I = 4*W_k + 8 integer ops, S = 16*W_k bytes of table/state traffic
+    (read table row, read availability, write availability, write the remaining
+    candidate set).  Weighted by the node mix per kind."""
+    info = puzzle.info()
+    nk = [info.nb_center, info.nb_border, info.nb_corner]
+    wk = [(4 * n + 31) // 32 for n in nk]
+    total = sum(kind_nodes) or 1
+    ops = sum((4 * wk[k] + 8) * kind_nodes[k] for k in range(3)) / total
+    byts = sum(16 * wk[k] * kind_nodes[k] for k in range(3)) / total
+    return ops, byts, [kn / total for kn in kind_nodes]
+
+
+_CPU_CACHE = {}
+
+
+def _cpu_puzzles():
+    """Oracle puzzles and their depth-12 prefixes (expanded once, on the CPU)."""
+    if not _CPU_CACHE:
+        from edge_matching_puzzle_b200.puzzle import generate
+        from oracle.oracle import OraclePuzzle
+        for s in SEEDS:
+            pz = generate(WIDTH, HEIGHT, BORDER, INTERIOR, s)
+            op = OraclePuzzle(WIDTH, HEIGHT, pz.colors)
+            count, _, _, pref = op.expand(DEPTH, max_prefixes=1 << 62)
+            _CPU_CACHE[s] = (op, count, pref)
+    return _CPU_CACHE
+
+
+def cpu_sample(threads: int, first: int, stride: int):
+    """Oracle (CPU restatement of emp_strategy) over the subtrees first, first+stride, ...
+    of the depth-12 prefixes of every workload puzzle.  Returns (nodes, seconds, kinds,
+    subtrees); only the subtree walks are timed."""
+    import ctypes
+    nodes = 0
+    seconds = 0.0
+    kinds = [0, 0, 0]
+    subtrees = 0
+    for s in SEEDS:
+        op, count, pref = _cpu_puzzles()[s]
+        sel = list(range(first, count, stride))
+        if not sel:
+            continue
+        buf = (ctypes.c_uint16 * (len(sel) * DEPTH))()
+        for i, j in enumerate(sel):
+            buf[i * DEPTH:(i + 1) * DEPTH] = pref[j * DEPTH:(j + 1) * DEPTH]
+        t0 = time.perf_counter()
+        nn, ss, kn = op.subtrees_parallel(buf, DEPTH, 0, len(sel), threads, kinds=True)
+        seconds += time.perf_counter() - t0
+        nodes += nn
+        kinds = [a + b for a, b in zip(kinds, kn)]
+        subtrees += len(sel)
+    return nodes, seconds, kinds, subtrees
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    nodes = seconds = 0.0
+    steps = []
+    for i in range(args.warmup + args.steps):
+        n, sec, _, sub = cpu_sample(threads, i, CPU_STRIDE * 2)
+        if i >= args.warmup:
+            nodes += n
+            seconds += sec
+            steps.append(sec)
+    value = nodes / seconds
+    out = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * statistics.mean(steps),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+        "config": {"workload": WORKLOAD + f"; each step a 1/{CPU_STRIDE * 2} sample of the subtrees"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"subtrees i, i+{CPU_STRIDE * 2}, ... (step i) of the 16 workload puzzles, "
+                                   f"oracle restatement of emp_strategy, one pthread per core"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--full", action="store_true", help="run all slices (the complete count) and print per-seed totals")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
+    args = ap.parse_args()
+    rank = env_int("RANK", 0)
+    world = env_int("WORLD_SIZE", 1)
+    local_rank = env_int("LOCAL_RANK", 0)
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import torch
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local_rank))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    from edge_matching_puzzle_b200 import native
+    puzzles = make_puzzles()
+    plan = native.BtPlan(puzzles, split_depth=DEPTH, device=local_rank)
+    total_subtrees = plan.subtrees()
+    flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.int32, device="cuda")
+    start_ev = torch.cuda.Event(enable_timing=True)
+    end_ev = torch.cuda.Event(enable_timing=True)
+
+    def slice_count(s):
+        return (total_subtrees - s + SLICES - 1) // SLICES if s < total_subtrees else 0
+
+    if args.full:
+        # the complete count of every workload puzzle in one run (all subtrees)
+        full_plan = native.BtPlan(puzzles, split_depth=DEPTH, device=local_rank)
+        full_plan.run()
+        res = full_plan.results()
+        if rank == 0:
+            for s, r in zip(SEEDS, res):
+                print(json.dumps({"seed": s, "nodes": r.nodes, "solutions": r.solutions,
+                                  "first_solution": list(r.first_solution)[:WIDTH * HEIGHT] if r.has_first_solution
+                                  else None}), flush=True)
+            nodes_all = sum(r.nodes for r in res)
+            print(json.dumps({"full_count_s": res[0].kernel_ms / 1000, "nodes": nodes_all,
+                              "placements_per_s": nodes_all / (res[0].kernel_ms / 1000), "rounds": res[0].rounds}),
+                  flush=True)
+        return
+
+    # ---------------- device-resident throughput ----------------
+    nodes = 0
+    ms = 0.0
+    busy = 0.0
+    rounds = 0
+    records = 0
+    launches = 0
+    step_ms = []
+    dev_index = torch.cuda.current_device()
+    sampler = ClockSampler(dev_index)
+    for i in range(args.warmup + args.steps):
+        s = (i * world + rank) % SLICES
+        if i == args.warmup:
+            sampler.__enter__()
+        flush.add_(1)  # writes 252 MB: evicts L2 between steps
+        barrier()
+        start_ev.record()
+        plan.select(s, SLICES, slice_count(s))
+        plan.run()
+        end_ev.record()
+        barrier()
+        res = plan.results()
+        if i >= args.warmup:
+            t = start_ev.elapsed_time(end_ev)
+            step_ms.append(t)
+            ms += t
+            nodes += sum(r.nodes for r in res)
+            busy += res[0].dfs_busy_ms
+            rounds += res[0].rounds
+            records += res[0].work_records + res[0].handed_back
+            launches += 2 + res[0].rounds  # make_records + reset + one DFS launch per round
+    sampler.__exit__()
+    clocks = sampler.summary()
+    if dist is not None:
+        t = torch.tensor([ms, float(nodes)], dtype=torch.float64, device="cuda")
+        mx = t.clone()
+        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        ms_max, nodes_all = mx[0].item(), t[1].item()
+    else:
+        ms_max, nodes_all = ms, float(nodes)
+    value = nodes_all / (ms_max / 1000.0)
+
+    # ---------------- end to end through the public one-shot call ----------------
+    e2e = None
+    if not args.no_e2e:
+        from edge_matching_puzzle_b200.puzzle import generate
+        host_inputs = [generate(WIDTH, HEIGHT, BORDER, INTERIOR, s) for s in SEEDS]
+        e_nodes = 0
+        e_sec = 0.0
+        h2d = d2h = 0
+        for i in range(1 + args.steps):
+            s = (i * world + rank) % SLICES
+            barrier()
+            t0 = time.perf_counter()
+            hp = [native.NativePuzzle(WIDTH, HEIGHT, p.colors) for p in host_inputs]
+            res = native.bt_count_batch(hp, split_depth=DEPTH, device=local_rank, sample_first=s,
+                                        sample_stride=SLICES)
+            torch.cuda.synchronize()
+            dt = time.perf_counter() - t0
+            if i >= 1:
+                e_nodes += sum(r.nodes for r in res)
+                e_sec += dt
+                tables = sum(p.table_bytes() for p in hp)
+                h2d = tables + 12 * len(hp)  # table blobs, blob offsets, first parents
+                d2h = (8 * (2 * len(hp) + DEPTH + res[0].rounds) + 528 * len(hp) + 8)
+            for p in hp:
+                p.close()
+        if dist is not None:
+            t = torch.tensor([e_sec, float(e_nodes)], dtype=torch.float64, device="cuda")
+            mx = t.clone()
+            dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+            dist.all_reduce(t, op=dist.ReduceOp.SUM)
+            e_sec, e_nodes = mx[0].item(), t[1].item()
+        e2e = {"value": e_nodes / e_sec, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h}
+
+    # ---------------- CPU baseline (oracle) and algorithmic work ----------------
+    peaks, peak_kind = measured_peaks()
+    cpu = None
+    kinds = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        threads = os.cpu_count() or 1
+        cn, csec, kinds, csub = cpu_sample(threads, 0, CPU_STRIDE)
+        cpu = {"value": cn / csec, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": f"{csub} depth-{DEPTH} subtrees (every {CPU_STRIDE}th) of the 16 workload puzzles, "
+                         f"{cn} placements, CPU oracle (restatement of emp_strategy), one pthread per core"}
+    if rank == 0:
+        if kinds is None:
+            kinds = [85, 14, 1]
+        ops, byts, mix = algorithmic_work(kinds, puzzles[0])
+        launch_ms = busy / max(rounds, 1)
+        placements_per_launch = nodes / max(rounds, 1)
+        sm_clock = (clocks or {}).get("sm_max_mhz") or peaks.get("sm_max_mhz", 1965.0)
+        rec_bytes = 4 * plan.rec_words()
+        dram_alg = records * rec_bytes / max(rounds, 1)  # work records read and written per launch
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "puzzles": len(SEEDS), "split_depth": DEPTH,
+                       "subtrees_per_step": total_subtrees // SLICES, "parallelism": f"{world} GPU(s), disjoint slices",
+                       "l2": "flushed between steps (252 MB write)"},
+            "gpu_launches": launches,
+            "roofline": {"bound": "hbm", "achieved": dram_alg / (launch_ms / 1000) / 1e9,
+                         "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                         "frac": dram_alg / (launch_ms / 1000) / 1e9 / peaks["hbm_gbs"], "traffic": None,
+                         "peak_source": peak_kind,
+                         "note": "dfs_kernel keeps its state on chip; DRAM only carries work records, so the "
+                                 "on-chip roofline below is the binding one"},
+            "roofline_onchip": {
+                "kernel": "dfs_kernel", "launch_ms": launch_ms, "placements_per_launch": placements_per_launch,
+                "int_ops_per_placement": ops, "smem_bytes_per_placement": byts, "node_mix_center_border_corner": mix,
+                "int_issue": {"achieved_tops": placements_per_launch * ops / (launch_ms / 1000) / 1e12,
+                              "peak_tops": 148 * 4 * 32 * sm_clock * 1e6 / 1e12},
+                "smem": {"achieved_gbs": placements_per_launch * byts / (launch_ms / 1000) / 1e9,
+                         "peak_gbs": 148 * 128 * sm_clock * 1e6 / 1e9},
+            },
+            "clocks": clocks,
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+            "dfs": {"rounds_per_step": rounds / args.steps, "busy_frac": busy / ms if ms else None},
+        }
+        oc = out["roofline_onchip"]
+        oc["int_issue"]["frac"] = oc["int_issue"]["achieved_tops"] / oc["int_issue"]["peak_tops"]
+        oc["smem"]["frac"] = oc["smem"]["achieved_gbs"] / oc["smem"]["peak_gbs"]
+        print(json.dumps(out), flush=True)
+    plan.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

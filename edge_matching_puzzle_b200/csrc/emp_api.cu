@@ -105,14 +105,18 @@ struct emp_bt_plan_t {
     uint64_t n_all = 0, n_init = 0;
     bool sampled = false;
     std::vector<unsigned long long> exp_nodes, exp_sols;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, evr0 = nullptr, evr1 = nullptr;
     bool ran = false;
     uint32_t rounds = 0;
+    double busy_ms = 0;
+    uint64_t records_in = 0, records_out = 0;
 
     ~emp_bt_plan_t()
     {
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
+        if (evr0) cudaEventDestroy(evr0);
+        if (evr1) cudaEventDestroy(evr1);
     }
 
     emp::BtLaunch launch() const
@@ -267,6 +271,8 @@ extern "C" emp_status emp_bt_plan_create(const emp_puzzle* puzzles, uint32_t cou
     CUDA_TRY(pl->prefix_out.alloc(sizeof(uint16_t) * 256));
     CUDA_TRY(cudaEventCreate(&pl->ev0));
     CUDA_TRY(cudaEventCreate(&pl->ev1));
+    CUDA_TRY(cudaEventCreate(&pl->evr0));
+    CUDA_TRY(cudaEventCreate(&pl->evr1));
     EMP_TRY(expand(*pl));
     // launch geometry: as many blocks per SM as shared memory allows
     cudaDeviceProp prop;
@@ -338,18 +344,28 @@ extern "C" emp_status emp_bt_plan_run(emp_bt_plan plan, void* stream)
     DeviceBuffer* out = &plan->rec_a;
     DeviceBuffer* spare = &plan->rec_b;
     plan->rounds = 0;
+    plan->busy_ms = 0;
+    plan->records_in = 0;
+    plan->records_out = 0;
     while (n_in) {
+        plan->records_in += n_in;
         CUDA_TRY(cudaMemsetAsync(plan->counters.p, 0, plan->counters.bytes, st));
         P.in_rec = in;
         P.n_in = n_in;
         P.out_rec = out->as<uint32_t>();
+        CUDA_TRY(cudaEventRecord(plan->evr0, st));
         CUDA_TRY(emp::launch_dfs(P, plan->blocks, plan->threads, st));
+        CUDA_TRY(cudaEventRecord(plan->evr1, st));
         ++plan->rounds;
         unsigned long long tail = 0;
         CUDA_TRY(cudaMemcpyAsync(&tail, plan->counters.as<unsigned long long>() + 1, sizeof(tail),
                                  cudaMemcpyDeviceToHost, st));
         CUDA_TRY(cudaStreamSynchronize(st));
+        float rms = 0;
+        CUDA_TRY(cudaEventElapsedTime(&rms, plan->evr0, plan->evr1));
+        plan->busy_ms += rms;
         n_in = std::min<uint64_t>(tail, plan->capacity);
+        plan->records_out += n_in;
         in = out->as<uint32_t>();
         std::swap(out, spare);
         if (plan->rounds > 100000) return fail(EMP_ERR_CUDA, "emp_bt_plan_run: too many rounds");
@@ -388,6 +404,9 @@ extern "C" emp_status emp_bt_plan_results(emp_bt_plan plan, emp_bt_result* resul
         r.status = aborted ? EMP_INCOMPLETE : EMP_OK;
         r.kernel_ms = ms;
         r.rounds = plan->rounds;
+        r.dfs_busy_ms = plan->busy_ms;
+        r.work_records = plan->records_in;
+        r.handed_back = plan->records_out;
         for (uint32_t pos = 0; pos < 256; ++pos) r.first_solution[pos] = 0xFFFFFFFFu;
         if (rec[i].has && !rec[i].missed) {
             for (uint32_t l = 0; l < pz->model.n; ++l) {
@@ -444,6 +463,12 @@ extern "C" emp_status emp_bt_count_batch(const emp_puzzle* puzzles, uint32_t cou
     emp_status s = emp_bt_plan_create(puzzles, count, config, &plan);
     if (s != EMP_OK) return s;
     std::unique_ptr<emp_bt_plan_t> guard(plan);
+    if (config && config->sample_stride) {
+        const uint64_t first = config->sample_first, stride = config->sample_stride;
+        const uint64_t n = first < plan->n_all ? (plan->n_all - first + stride - 1) / stride : 0;
+        s = emp_bt_plan_select(plan, first, stride, n);
+        if (s != EMP_OK) return s;
+    }
     s = emp_bt_plan_run(plan, nullptr);
     if (s != EMP_OK) return s;
     s = emp_bt_plan_results(plan, results);

@@ -52,7 +52,9 @@ class BtConfig(ctypes.Structure):
         ("device", ctypes.c_int32),
         ("keep_subtree_counts", ctypes.c_uint32),
         ("split_budget", ctypes.c_uint32),
-        ("reserved", ctypes.c_uint32 * 6),
+        ("sample_stride", ctypes.c_uint32),
+        ("sample_first", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32 * 4),
     ]
 
 
@@ -70,6 +72,9 @@ class BtResult(ctypes.Structure):
         ("total_ms", ctypes.c_double),
         ("rounds", ctypes.c_uint32),
         ("reserved", ctypes.c_uint32),
+        ("dfs_busy_ms", ctypes.c_double),
+        ("work_records", ctypes.c_uint64),
+        ("handed_back", ctypes.c_uint64),
     ]
 
 
@@ -158,6 +163,14 @@ class NativePuzzle:
         check(load().emp_puzzle_export_tables(self.handle, buf, words.value, ctypes.byref(words)))
         return list(buf)
 
+    def max_kind_words(self) -> int:
+        """64-bit words of the widest kind bitfield (4 bits per piece)."""
+        i = self.info()
+        return (4 * max(i.nb_center, i.nb_border, i.nb_corner) + 63) // 64
+
+    def table_bytes(self) -> int:
+        return 4 * len(self.export_tables())
+
     def info(self) -> PuzzleInfo:
         i = PuzzleInfo()
         check(load().emp_puzzle_get_info(self.handle, ctypes.byref(i)))
@@ -226,6 +239,12 @@ class BtPlan:
         buf = (ctypes.c_uint16 * depth)()
         check(load().emp_bt_plan_subtree_prefix(self.handle, index, buf, depth))
         return list(buf)
+
+    def rec_words(self) -> int:
+        """32-bit words per work record (header, prefix, remaining set)."""
+        n = max(p.n for p in self.puzzles)
+        kw = max(p.max_kind_words() for p in self.puzzles)
+        return 4 + (n + 1) // 2 + 2 * kw
 
     def close(self):
         if getattr(self, "handle", None):

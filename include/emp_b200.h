@@ -108,7 +108,10 @@ typedef struct emp_bt_config {
     uint32_t split_budget;       /* once a round's queue is empty, a thread that spent this many
                                     DFS steps on its work record hands the rest back as new records
                                     for the next round; 0 = default (2048) */
-    uint32_t reserved[6];
+    uint32_t sample_stride;      /* emp_bt_count[_batch]: count only subtrees sample_first,
+                                    sample_first+sample_stride, ...; 0 = all subtrees */
+    uint32_t sample_first;
+    uint32_t reserved[4];
 } emp_bt_config;
 
 typedef struct emp_bt_result {
@@ -124,10 +127,16 @@ typedef struct emp_bt_result {
     double total_ms;             /* whole call, host clock */
     uint32_t rounds;             /* DFS rounds (work handed back between rounds) */
     uint32_t reserved;
+    double dfs_busy_ms;          /* sum of the DFS launches' device times (no gaps between rounds) */
+    uint64_t work_records;       /* work records read by the DFS launches (all rounds) */
+    uint64_t handed_back;        /* work records written back for a next round */
 } emp_bt_result;
 
 /* Exhaustive count of one puzzle: every solution and every placement of the
- * reference's search (position 0 keeps its first candidate, emp_strategy.h:389). */
+ * reference's search (position 0 keeps its first candidate, emp_strategy.h:389).
+ * With config->sample_stride set, only the sampled subtrees are counted and
+ * nodes/solutions hold their counts (expansion_nodes still reports the levels
+ * below the split depth). */
 emp_status emp_bt_count(emp_puzzle puzzle, const emp_bt_config *config, emp_bt_result *result);
 
 /* Same for many puzzles in one persistent launch; results[i] per puzzle. */

@@ -550,7 +550,7 @@ static void bt_replay(bt_state *s, const uint16_t *prefix, uint32_t depth)
 }
 
 static int bt_subtree_state(bt_state *s, const uint16_t *prefix, uint32_t depth, uint64_t node_limit,
-                            uint64_t *nodes_out, uint64_t *sols_out)
+                            uint64_t *nodes_out, uint64_t *sols_out, uint64_t *kind_nodes)
 {
     const op_puzzle *p = s->p;
     uint32_t n = s->n;
@@ -569,6 +569,7 @@ static int bt_subtree_state(bt_state *s, const uint16_t *prefix, uint32_t depth,
             s->piece_info[idx] = p->binary[s->kind[idx]][t];
             bt_select(s, idx, t);
             ++nodes;
+            if (kind_nodes) ++kind_nodes[s->kind[idx]];
             if (idx == n - 1) ++sols;
             ++idx;
             bt_compute(s, idx);
@@ -589,7 +590,7 @@ int op_bt_subtree(op_puzzle *p, const uint32_t *order, const uint16_t *prefix, u
     build_table(p);
     bt_state s;
     bt_init(&s, p, order);
-    int r = bt_subtree_state(&s, prefix, depth, node_limit, nodes, solutions);
+    int r = bt_subtree_state(&s, prefix, depth, node_limit, nodes, solutions, NULL);
     bt_free(&s);
     return r;
 }
@@ -695,6 +696,7 @@ typedef struct {
     pthread_mutex_t *mu;
     uint64_t nodes, sols;
     uint64_t *per_nodes, *per_sols, begin;
+    uint64_t kind_nodes[3];
 } par_job;
 
 static void *par_worker(void *arg)
@@ -706,7 +708,7 @@ static void *par_worker(void *arg)
         uint64_t i = __atomic_fetch_add(j->next, 1, __ATOMIC_RELAXED);
         if (i >= j->end) break;
         uint64_t nn = 0, ss = 0;
-        bt_subtree_state(&s, j->prefixes + i * j->depth, j->depth, 0, &nn, &ss);
+        bt_subtree_state(&s, j->prefixes + i * j->depth, j->depth, 0, &nn, &ss, j->kind_nodes);
         j->nodes += nn;
         j->sols += ss;
         if (j->per_nodes) j->per_nodes[i - j->begin] = nn;
@@ -719,7 +721,7 @@ static void *par_worker(void *arg)
 int op_bt_subtrees_parallel(op_puzzle *p, const uint32_t *order, const uint16_t *prefixes,
                             uint32_t depth, uint64_t begin, uint64_t end, int nthreads,
                             uint64_t *nodes, uint64_t *solutions, uint64_t *per_nodes,
-                            uint64_t *per_solutions)
+                            uint64_t *per_solutions, uint64_t *kind_nodes)
 {
     build_table(p);
     if (nthreads < 1) nthreads = 1;
@@ -738,6 +740,8 @@ int op_bt_subtrees_parallel(op_puzzle *p, const uint32_t *order, const uint16_t 
         pthread_join(th[t], NULL);
         nn += jobs[t].nodes;
         ss += jobs[t].sols;
+        if (kind_nodes)
+            for (int k = 0; k < 3; ++k) kind_nodes[k] += jobs[t].kind_nodes[k];
     }
     *nodes = nn;
     *solutions = ss;

@@ -98,12 +98,14 @@ int op_bt_subtree(op_puzzle *p, const uint32_t *order, const uint16_t *prefix,
                   uint64_t *solutions);
 
 /* Multi-threaded subtree counting over prefixes [begin,end) with nthreads
- * pthreads; per-prefix node/solution counts are optional outputs. */
+ * pthreads; per-prefix node/solution counts and the nodes per position kind
+ * (kind_nodes[3], added to) are optional outputs. */
 int op_bt_subtrees_parallel(op_puzzle *p, const uint32_t *order,
                             const uint16_t *prefixes, uint32_t depth,
                             uint64_t begin, uint64_t end, int nthreads,
                             uint64_t *nodes, uint64_t *solutions,
-                            uint64_t *per_nodes, uint64_t *per_solutions);
+                            uint64_t *per_nodes, uint64_t *per_solutions,
+                            uint64_t *kind_nodes);
 
 /* Knuth random-probe estimate of the exhaustive tree size (sizing only). */
 double op_bt_estimate(op_puzzle *p, const uint32_t *order, uint32_t probes,

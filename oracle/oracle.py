@@ -85,7 +85,7 @@ def lib():
                                     ctypes.POINTER(u64), ctypes.POINTER(u64)]
         L.op_bt_subtrees_parallel.argtypes = [vp, ctypes.POINTER(u32), ctypes.POINTER(ctypes.c_uint16), u32, u64, u64,
                                               ctypes.c_int, ctypes.POINTER(u64), ctypes.POINTER(u64),
-                                              ctypes.POINTER(u64), ctypes.POINTER(u64)]
+                                              ctypes.POINTER(u64), ctypes.POINTER(u64), ctypes.POINTER(u64)]
         L.op_bt_estimate.restype = ctypes.c_double
         L.op_bt_estimate.argtypes = [vp, ctypes.POINTER(u32), u32, u64, ctypes.POINTER(ctypes.c_double)]
         L.op_gm_run.argtypes = [vp, u64, ctypes.POINTER(GmResult)]
@@ -174,15 +174,19 @@ class OraclePuzzle:
         return nn.value, ss.value, st
 
     def subtrees_parallel(self, prefixes, depth: int, begin: int, end: int, threads: int, order=None,
-                          per_item: bool = False):
+                          per_item: bool = False, kinds: bool = False):
         nn, ss = ctypes.c_uint64(), ctypes.c_uint64()
         pn = (ctypes.c_uint64 * max(1, end - begin))() if per_item else None
         ps = (ctypes.c_uint64 * max(1, end - begin))() if per_item else None
+        kn = (ctypes.c_uint64 * 3)()
         lib().op_bt_subtrees_parallel(self._p, self._order(order), prefixes, depth, begin, end, threads,
-                                      ctypes.byref(nn), ctypes.byref(ss), pn, ps)
+                                      ctypes.byref(nn), ctypes.byref(ss), pn, ps, kn)
+        out = (nn.value, ss.value)
         if per_item:
-            return nn.value, ss.value, list(pn), list(ps)
-        return nn.value, ss.value
+            out = out + (list(pn), list(ps))
+        if kinds:
+            out = out + (list(kn),)
+        return out
 
     def estimate(self, probes: int, seed: int = 1, order=None) -> float:
         return lib().op_bt_estimate(self._p, self._order(order), probes, seed, None)
