@@ -95,7 +95,7 @@ struct emp_bt_plan_t {
     emp_bt_config cfg{};
     int device = 0;
     uint32_t depth = 0, max_levels = 0, max_avail = 0, max_kw = 0;
-    uint32_t threads = 128, blocks = 0, rec_words = 0;
+    uint32_t threads = 128, blocks = 0, rec_words = 0, smem_tab_words = 0;
     uint64_t capacity = 0, budget = 0;
     DeviceBuffer tables, poff;
     DeviceBuffer prefixes, prefix_puzzle;     // split-depth prefixes (all)
@@ -129,6 +129,7 @@ struct emp_bt_plan_t {
         P.max_avail_words = max_avail;
         P.max_kw = max_kw;
         P.spill = spill.as<uint64_t>();
+        P.smem_tab_words = smem_tab_words;
         P.rec_words = rec_words;
         P.rec_r_off = rec_words - 2 * max_kw;
         P.out_capacity = capacity;
@@ -274,23 +275,38 @@ extern "C" emp_status emp_bt_plan_create(const emp_puzzle* puzzles, uint32_t cou
     CUDA_TRY(cudaEventCreate(&pl->evr0));
     CUDA_TRY(cudaEventCreate(&pl->evr1));
     EMP_TRY(expand(*pl));
-    // launch geometry: as many blocks per SM as shared memory allows
+    // hot tables in shared memory when the plan holds one puzzle
+    const uint32_t hot = (pl->puzzles[0]->tables.blob[26] + 3u) & ~3u;
+    const bool want_smem = pl->cfg.table_placement == 2 || (pl->cfg.table_placement == 0 && count == 1);
+    pl->smem_tab_words = (want_smem && count == 1 && hot * 4 <= 64 * 1024) ? hot : 0;
+    if (pl->cfg.table_placement == 2 && !pl->smem_tab_words)
+        return fail(EMP_ERR_UNSUPPORTED, "tables can only be staged in shared memory for a single puzzle up to 64 KB");
+    // launch geometry: the block size with the most resident warps per SM
     cudaDeviceProp prop;
     CUDA_TRY(cudaGetDeviceProperties(&prop, pl->device));
-    pl->threads = pl->cfg.threads_per_block ? pl->cfg.threads_per_block : 128;
-    if (pl->threads % 32 || pl->threads > 256)
-        return fail(EMP_ERR_INVALID, "threads_per_block must be a multiple of 32 up to 256");
-    const size_t smem = emp::dfs_smem_bytes(pl->max_levels, pl->max_avail, pl->threads);
-    if (smem > static_cast<size_t>(prop.sharedMemPerBlockOptin))
+    if (pl->max_kw > 16) return fail(EMP_ERR_UNSUPPORTED, "puzzle kinds wider than 16 64-bit words");
+    std::vector<uint32_t> candidates;
+    if (pl->cfg.threads_per_block) candidates.push_back(pl->cfg.threads_per_block);
+    else candidates = {64, 128, 256};
+    int best_warps = 0;
+    for (uint32_t threads : candidates) {
+        const void* fn = emp::dfs_kernel_symbol(pl->max_kw, pl->smem_tab_words != 0, threads);
+        if (!fn) return fail(EMP_ERR_INVALID, "threads_per_block must be 64, 128 or 256");
+        const size_t smem = emp::dfs_smem_bytes(pl->max_levels, pl->max_avail, threads, pl->smem_tab_words);
+        if (smem > static_cast<size_t>(prop.sharedMemPerBlockOptin)) continue;
+        CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+        int per_sm = 0;
+        CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, static_cast<int>(threads), smem));
+        if (pl->cfg.blocks_per_sm) per_sm = std::min<int>(per_sm, static_cast<int>(pl->cfg.blocks_per_sm));
+        const int warps = per_sm * static_cast<int>(threads / 32);
+        if (per_sm >= 1 && warps > best_warps) {
+            best_warps = warps;
+            pl->threads = threads;
+            pl->blocks = static_cast<uint32_t>(per_sm) * static_cast<uint32_t>(prop.multiProcessorCount);
+        }
+    }
+    if (!best_warps)
         return fail(EMP_ERR_UNSUPPORTED, "per-thread DFS state does not fit shared memory; use fewer threads per block");
-    CUDA_TRY(cudaFuncSetAttribute(emp::dfs_kernel_symbol(pl->max_kw), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  static_cast<int>(smem)));
-    int per_sm = 0;
-    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, emp::dfs_kernel_symbol(pl->max_kw),
-                                                           static_cast<int>(pl->threads), smem));
-    if (per_sm < 1) return fail(EMP_ERR_UNSUPPORTED, "DFS kernel cannot be resident with this configuration");
-    if (pl->cfg.blocks_per_sm) per_sm = std::min<int>(per_sm, static_cast<int>(pl->cfg.blocks_per_sm));
-    pl->blocks = static_cast<uint32_t>(per_sm) * static_cast<uint32_t>(prop.multiProcessorCount);
     CUDA_TRY(pl->spill.alloc(sizeof(uint64_t) * static_cast<size_t>(pl->blocks) * pl->threads * pl->max_levels *
                              pl->max_kw));
     // round queues: room for every resident thread to hand back a full path twice
@@ -455,10 +471,11 @@ extern "C" void emp_bt_plan_destroy(emp_bt_plan plan)
     }
 }
 
-extern "C" emp_status emp_bt_count_batch(const emp_puzzle* puzzles, uint32_t count, const emp_bt_config* config,
-                                         emp_bt_result* results)
+namespace {
+
+emp_status count_one_plan(const emp_puzzle* puzzles, uint32_t count, const emp_bt_config* config,
+                          emp_bt_result* results)
 {
-    const auto t0 = std::chrono::steady_clock::now();
     emp_bt_plan plan = nullptr;
     emp_status s = emp_bt_plan_create(puzzles, count, config, &plan);
     if (s != EMP_OK) return s;
@@ -471,9 +488,28 @@ extern "C" emp_status emp_bt_count_batch(const emp_puzzle* puzzles, uint32_t cou
     }
     s = emp_bt_plan_run(plan, nullptr);
     if (s != EMP_OK) return s;
-    s = emp_bt_plan_results(plan, results);
+    return emp_bt_plan_results(plan, results);
+}
+
+}  // namespace
+
+extern "C" emp_status emp_bt_count_batch(const emp_puzzle* puzzles, uint32_t count, const emp_bt_config* config,
+                                         emp_bt_result* results)
+{
+    emp::clear_error();
+    if (!puzzles || !count || !results) return fail(EMP_ERR_INVALID, "emp_bt_count_batch: no puzzle");
+    const auto t0 = std::chrono::steady_clock::now();
+    // Puzzles with big trees run one plan each (tables staged in shared memory);
+    // many small puzzles share one launch (tables read from global memory).
+    bool separate = count <= 64 && (!config || config->table_placement != 1);
+    for (uint32_t i = 0; i < count && separate; ++i) separate = puzzles[i] && puzzles[i]->model.n >= 36;
+    emp_status s = EMP_OK;
+    if (separate && count > 1) {
+        for (uint32_t i = 0; i < count && s == EMP_OK; ++i) s = count_one_plan(&puzzles[i], 1, config, &results[i]);
+    } else {
+        s = count_one_plan(puzzles, count, config, results);
+    }
     if (s != EMP_OK) return s;
-    guard.reset();
     const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     bool incomplete = false;
     for (uint32_t i = 0; i < count; ++i) {

@@ -73,12 +73,7 @@ __global__ void expand_kernel(BtLaunch P, const uint16_t* __restrict__ parents,
         if (level < n) {
             const LevelDesc d = load_desc(tb, desc_off, level);
             const uint32_t kw = d.kw();
-            uint32_t row = d.d2;
-            if (d.arity() >= 1) {
-                const uint32_t ca = facing_colour(stk[d.level_a()], d.side_a());
-                const uint32_t cb = d.arity() >= 2 ? facing_colour(stk[d.level_b()], d.side_b()) : 0u;
-                row += ((d.arity() >= 2 ? ca * ncol + cb : ca) * kw) * 2;
-            }
+            const uint32_t row = d.row(stk[d.level_a()], stk[d.level_b()]);
             uint64_t R[kMaxKindWords];
             for (uint32_t w = 0; w < kw; ++w) R[w] = ldg64(tb + row + 2 * w) & av[d.aoff() + w];
             for (uint32_t j = 0; j < d.nextra(); ++j) {
@@ -202,42 +197,88 @@ __global__ void scan_apply(const uint32_t* __restrict__ in, uint64_t n, const ui
 // [3] puzzle | spilled<<16 | empty<<17, [4..] transitions (u16 pairs), then
 // the remaining set of level len (max_kw 64-bit words as u32 pairs).
 //
-// Per-thread state in shared memory, thread-interleaved (a warp touching its
-// own entries hits distinct banks):
-//   stk[L*T + tid] = t << 21 | spilled << 20 | colours of the placed piece
+// Per-thread state in shared memory, thread-interleaved with a compile-time
+// block size T (a warp touching its own entries hits distinct banks and every
+// address is base + immediate):
+//   stk[L*T + tid] = more<<31 | t<<21 | spilled<<20 | colours of the placed piece
+//                    (more: candidates remained after t when it was placed)
 //   av[w*T + tid]  = 64-bit availability words of the three kinds
 struct ThreadItem {
     uint64_t orig;
     const uint32_t* tb;
-    uint32_t pz, n, ncol, desc_off, L, base, start, spilled;
+    uint32_t pz, n, desc_off, L, base, start, spilled;
+    bool pop;  // the current level is known to be exhausted: go up without scanning
     uint64_t nodes, sols, steps;
     bool active;
 };
+
+// Table access: SM = the plan's single puzzle has its hot tables (header,
+// pair tables, level descriptors, transition info) staged in shared memory at
+// the start of the block's dynamic shared memory; otherwise every read goes
+// through the read-only data path from the global blob.
+extern __shared__ __align__(16) uint32_t g_smem[];
+
+template <bool SM>
+struct Tab;
+
+template <>
+struct Tab<true> {
+    static __device__ __forceinline__ uint32_t u32(const ThreadItem&, uint32_t off) { return g_smem[off]; }
+    static __device__ __forceinline__ uint64_t u64(const ThreadItem&, uint32_t off)
+    {
+        return reinterpret_cast<const unsigned long long*>(g_smem)[off >> 1];
+    }
+    static __device__ __forceinline__ LevelDesc desc(const ThreadItem& s, uint32_t L)
+    {
+        const uint4* d = reinterpret_cast<const uint4*>(g_smem + s.desc_off + 8 * L);
+        const uint4 a = d[0], b = d[1];
+        return LevelDesc{a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+    }
+};
+
+template <>
+struct Tab<false> {
+    static __device__ __forceinline__ uint32_t u32(const ThreadItem& s, uint32_t off) { return ldg(s.tb + off); }
+    static __device__ __forceinline__ uint64_t u64(const ThreadItem& s, uint32_t off) { return ldg64(s.tb + off); }
+    static __device__ __forceinline__ LevelDesc desc(const ThreadItem& s, uint32_t L)
+    {
+        return load_desc(s.tb, s.desc_off, L);
+    }
+};
+
+// 64-bit shift left whose amount saturates at 64 (PTX clamps shift amounts)
+__device__ __forceinline__ uint64_t shl_sat(uint64_t v, uint32_t n)
+{
+    uint64_t r;
+    asm("shl.b64 %0, %1, %2;" : "=l"(r) : "l"(v), "r"(n));
+    return r;
+}
 
 __device__ __forceinline__ uint32_t rec_t(const uint32_t* rec, uint32_t l)
 {
     return (rec[4 + (l >> 1)] >> (16 * (l & 1))) & 0xFFFFu;
 }
 
+template <bool SM, int T>
 __device__ __forceinline__ void load_record(const BtLaunch& P, ThreadItem& s, const uint32_t* rec, uint32_t* stk,
-                                            uint64_t* av, uint64_t* spill, uint32_t T, uint32_t tid)
+                                            uint64_t* av, uint64_t* spill)
 {
+    using TB = Tab<SM>;
     s.orig = static_cast<uint64_t>(rec[0]) | (static_cast<uint64_t>(rec[1]) << 32);
     const uint32_t len = rec[2] & 0xFFFFu;
     s.start = rec[2] >> 16;
     s.pz = rec[3] & 0xFFFFu;
     s.spilled = (rec[3] >> 16) & 1u;
     s.tb = P.tables + P.puzzle_offset[s.pz];
-    s.n = ldg(s.tb + H_N);
-    s.ncol = ldg(s.tb + H_NCOL);
-    s.desc_off = ldg(s.tb + H_DESC);
-    const uint32_t aw = ldg(s.tb + H_AWORDS), init = ldg(s.tb + H_INIT);
-    for (uint32_t w = 0; w < aw; ++w) av[w * T + tid] = ldg64(s.tb + init + 2 * w);
+    s.n = TB::u32(s, H_N);
+    s.desc_off = TB::u32(s, H_DESC);
+    const uint32_t aw = TB::u32(s, H_AWORDS), init = TB::u32(s, H_INIT);
+    for (uint32_t w = 0; w < aw; ++w) av[w * T] = ldg64(s.tb + init + 2 * w);
     for (uint32_t l = 0; l < len; ++l) {
-        const LevelDesc d = load_desc(s.tb, s.desc_off, l);
+        const LevelDesc d = TB::desc(s, l);
         const uint32_t t = rec_t(rec, l);
-        av[(d.aoff() + (t >> 6)) * T + tid] &= ~(0xFull << (t & 60u));
-        stk[l * T + tid] = (t << 21) | (ldg(s.tb + d.d5 + t) & 0xFFFFFu);
+        av[(d.aoff() + (t >> 6)) * T] &= ~(0xFull << (t & 60u));
+        stk[l * T] = (t << 21) | (TB::u32(s, d.d5 + t) & 0xFFFFFu);
     }
     if (s.spilled) {
         const uint32_t* R = rec + P.rec_r_off;
@@ -246,6 +287,7 @@ __device__ __forceinline__ void load_record(const BtLaunch& P, ThreadItem& s, co
     }
     s.L = len;
     s.base = len;
+    s.pop = false;
     s.nodes = 0;
     s.sols = 0;
     s.steps = 0;
@@ -254,11 +296,11 @@ __device__ __forceinline__ void load_record(const BtLaunch& P, ThreadItem& s, co
 
 // Candidate words of level L (not yet masked by the resume bit): the level's
 // pair-table row (frame sides & placed neighbours) & availability, or the
-// spilled remaining set.
-template <int KW>
+// spilled remaining set.  stk/av are this thread's columns.
+template <int KW, bool SM, int T>
 __device__ __forceinline__ void level_candidates(const BtLaunch& P, const ThreadItem& s, const LevelDesc& d,
                                                  uint32_t L, bool spilled, const uint32_t* stk, const uint64_t* av,
-                                                 const uint64_t* spill, uint32_t T, uint32_t tid, uint64_t* x)
+                                                 const uint64_t* spill, uint64_t* x)
 {
     const uint32_t kw = d.kw();
     if (spilled) {
@@ -267,20 +309,16 @@ __device__ __forceinline__ void level_candidates(const BtLaunch& P, const Thread
         for (int w = 0; w < KW; ++w) x[w] = (uint32_t)w < kw ? sp[w] : 0ull;
         return;
     }
-    uint32_t row = d.d2;
-    if (d.arity() >= 1) {
-        const uint32_t ca = facing_colour(stk[d.level_a() * T + tid], d.side_a());
-        const uint32_t cb = d.arity() >= 2 ? facing_colour(stk[d.level_b() * T + tid], d.side_b()) : 0u;
-        row += ((d.arity() >= 2 ? ca * s.ncol + cb : ca) * kw) * 2;
-    }
-    const uint32_t* r = s.tb + row;
+    const uint32_t row = d.row(stk[d.level_a() * T], stk[d.level_b() * T]);
+    const uint64_t* a = av + d.aoff() * T;
 #pragma unroll
-    for (int w = 0; w < KW; ++w) x[w] = (uint32_t)w < kw ? ldg64(r + 2 * w) & av[(d.aoff() + w) * T + tid] : 0ull;
+    for (int w = 0; w < KW; ++w) x[w] = (uint32_t)w < kw ? Tab<SM>::u64(s, row + 2 * w) & a[w * T] : 0ull;
     if (d.nextra()) {
+        const uint32_t ncol = Tab<SM>::u32(s, H_NCOL);
         for (uint32_t j = 0; j < d.nextra(); ++j) {
             const uint32_t sd = d.extra_side(j);
-            const uint32_t c = facing_colour(stk[d.extra_level(j) * T + tid], sd);
-            const uint32_t* sm = s.tb + d.d4 + ((sd * s.ncol + c) * kw) * 2;
+            const uint32_t c = facing_colour(stk[d.extra_level(j) * T], sd);
+            const uint32_t* sm = s.tb + d.d4 + ((sd * ncol + c) * kw) * 2;
 #pragma unroll
             for (int w = 0; w < KW; ++w)
                 if ((uint32_t)w < kw) x[w] &= ldg64(sm + 2 * w);
@@ -288,78 +326,105 @@ __device__ __forceinline__ void level_candidates(const BtLaunch& P, const Thread
     }
 }
 
-// First candidate at or after bit `start`; returns false when there is none.
+// Masks the words below bit `start`, finds the first candidate t and whether
+// more candidates follow it.  Returns false when there is none.
 template <int KW>
-__device__ __forceinline__ bool first_candidate(const uint64_t* x, uint32_t start, uint32_t* t)
+__device__ __forceinline__ bool first_candidate(uint64_t* x, uint32_t start, uint32_t* t, bool* more)
 {
-    const uint32_t sw = start >> 6;
-    const uint64_t head = ~0ull << (start & 63u);
     bool found = false;
     uint32_t fw = 0;
     uint64_t fx = 0;
 #pragma unroll
     for (int w = 0; w < KW; ++w) {
-        uint64_t v = x[w];
-        v = (uint32_t)w < sw ? 0ull : ((uint32_t)w == sw ? v & head : v);
-        if (!found && v) {
+        const int sh = static_cast<int>(start) - 64 * w;
+        x[w] &= shl_sat(~0ull, static_cast<uint32_t>(sh > 0 ? sh : 0));
+        if (!found && x[w]) {
             found = true;
             fw = w;
-            fx = v;
+            fx = x[w];
         }
     }
+    uint64_t rest = fx & (fx - 1);  // first word without t
+#pragma unroll
+    for (int w = 0; w < KW; ++w)
+        if ((uint32_t)w > fw) rest |= x[w];
+    *more = rest != 0;
     *t = fw * 64 + __ffsll(fx) - 1;
     return found;
 }
 
-// One step of emp_strategy::specific_run (include/emp_strategy.h:352-401)
-// inside the thread's record.  Returns false once the record is exhausted.
-template <int KW>
-__device__ __forceinline__ bool dfs_step(const BtLaunch& P, ThreadItem& s, uint32_t* stk, uint64_t* av,
-                                         uint64_t* spill, uint32_t T, uint32_t tid, bool* solved)
+// Goes up one level: gives back the piece placed there and resumes after it.
+template <bool SM, int T>
+__device__ __forceinline__ void pop_level(ThreadItem& s, const uint32_t* stk, uint64_t* av)
 {
-    const LevelDesc d = load_desc(s.tb, s.desc_off, s.L);
-    uint64_t x[KW];
-    level_candidates<KW>(P, s, d, s.L, s.spilled != 0, stk, av, spill, T, tid, x);
-    uint32_t t;
-    if (first_candidate<KW>(x, s.start, &t)) {
-        const uint32_t ti = ldg(s.tb + d.d5 + t);
-        const uint32_t kw = d.kw();
-        if ((ti >> 20) & 1u) {
-            // select_piece with an identical mask that clears other candidates
-            // (emp_position_strategy.h:197-200): the level keeps its exact
-            // remaining set from now on
-            if (!s.spilled) level_candidates<KW>(P, s, d, s.L, false, stk, av, spill, T, tid, x);
-            const uint32_t* ex = s.tb + d.d6 + t * kw * 2;
-            uint64_t* sp = spill + s.L * P.max_kw;
-#pragma unroll
-            for (int w = 0; w < KW; ++w)
-                if ((uint32_t)w < kw) sp[w] = x[w] & ldg64(ex + 2 * w);
-            s.spilled = 1;
-        }
-        av[(d.aoff() + (t >> 6)) * T + tid] &= ~(0xFull << (t & 60u));
-        stk[s.L * T + tid] = (t << 21) | (s.spilled << 20) | (ti & 0xFFFFFu);
-        ++s.nodes;
-        if (s.L == s.n - 1) {
-            // solution: count it, give the piece back, try the next candidate
-            ++s.sols;
-            *solved = true;
-            av[(d.aoff() + (t >> 6)) * T + tid] |= 0xFull << (t & 60u);
-            s.start = t + 1;
-        } else {
-            ++s.L;
-            s.start = 0;
-            s.spilled = 0;
-        }
-        return true;
-    }
-    if (s.L == s.base) return false;
     --s.L;
-    const uint32_t e = stk[s.L * T + tid];
-    const uint32_t tb = e >> 21;
+    const uint32_t e = stk[s.L * T];
+    const uint32_t t = (e >> 21) & 0x3FFu;
     s.spilled = (e >> 20) & 1u;
-    const LevelDesc dl = load_desc(s.tb, s.desc_off, s.L);
-    av[(dl.aoff() + (tb >> 6)) * T + tid] |= 0xFull << (tb & 60u);
-    s.start = tb + 1;
+    s.pop = !(e >> 31);
+    const LevelDesc dl = Tab<SM>::desc(s, s.L);
+    av[(dl.aoff() + (t >> 6)) * T] |= 0xFull << (t & 60u);
+    s.start = t + 1;
+}
+
+// One step of emp_strategy::specific_run (include/emp_strategy.h:352-401)
+// inside the thread's record: place the next candidate of the current level,
+// or go up one level (without scanning when the level is known exhausted).
+// Returns false once the record is exhausted.
+template <int KW, bool SM, int T>
+__device__ __forceinline__ bool dfs_step(const BtLaunch& P, ThreadItem& s, uint32_t* stk, uint64_t* av,
+                                         uint64_t* spill, bool* solved)
+{
+    if (!s.pop) {
+        const LevelDesc d = Tab<SM>::desc(s, s.L);
+        uint64_t x[KW];
+        level_candidates<KW, SM, T>(P, s, d, s.L, s.spilled != 0, stk, av, spill, x);
+        uint32_t t;
+        bool more;
+        if (first_candidate<KW>(x, s.start, &t, &more)) {
+            const uint32_t ti = Tab<SM>::u32(s, d.d5 + t);
+            if ((ti >> 20) & 1u) {
+                // select_piece with an identical mask that clears other candidates
+                // (emp_position_strategy.h:197-200): the level keeps its exact
+                // remaining set from now on
+                const uint32_t kw = d.kw();
+                if (!s.spilled) level_candidates<KW, SM, T>(P, s, d, s.L, false, stk, av, spill, x);
+                const uint32_t* ex = s.tb + d.d6 + t * kw * 2;
+                uint64_t* sp = spill + s.L * P.max_kw;
+                uint64_t rest = 0;
+#pragma unroll
+                for (int w = 0; w < KW; ++w)
+                    if ((uint32_t)w < kw) {
+                        sp[w] = x[w] & ldg64(ex + 2 * w);
+                        const int sh = static_cast<int>(t + 1) - 64 * w;
+                        rest |= sp[w] & shl_sat(~0ull, static_cast<uint32_t>(sh > 0 ? sh : 0));
+                    }
+                more = rest != 0;
+                s.spilled = 1;
+            }
+            uint64_t& aw = av[(d.aoff() + (t >> 6)) * T];
+            const uint64_t nib = 0xFull << (t & 60u);
+            aw &= ~nib;
+            stk[s.L * T] = (static_cast<uint32_t>(more) << 31) | (t << 21) | (s.spilled << 20) | (ti & 0xFFFFFu);
+            ++s.nodes;
+            if (s.L == s.n - 1) {
+                // solution: count it, give the piece back, try the next candidate
+                ++s.sols;
+                *solved = true;
+                aw |= nib;
+                s.start = t + 1;
+                s.pop = !more;
+            } else {
+                ++s.L;
+                s.start = 0;
+                s.spilled = 0;
+            }
+            return true;
+        }
+    }
+    // nothing left at this level: go up
+    if (s.L == s.base) return false;
+    pop_level<SM, T>(s, stk, av);
     return true;
 }
 
@@ -367,8 +432,8 @@ __device__ __forceinline__ bool dfs_step(const BtLaunch& P, ThreadItem& s, uint3
 // reference's visiting order (ascending candidate bit at every level) that is
 // its first solution.  The lock is held for a few hundred cycles; the wait for
 // it is bounded and a thread that gives up flags the record as unreliable.
-__device__ void record_solution(const BtLaunch& P, const ThreadItem& s, const uint32_t* stk, uint32_t T,
-                                uint32_t tid)
+template <int T>
+__device__ void record_solution(const BtLaunch& P, const ThreadItem& s, const uint32_t* stk)
 {
     FirstRecord* r = P.first_records + s.pz;
     atomicMin(&P.first_item[s.pz], (unsigned long long)s.orig);
@@ -389,7 +454,7 @@ __device__ void record_solution(const BtLaunch& P, const ThreadItem& s, const ui
     bool better = !r->has;
     if (!better) {
         for (uint32_t l = 0; l < s.n; ++l) {
-            const uint32_t mine = stk[l * T + tid] >> 21, theirs = r->t[l];
+            const uint32_t mine = (stk[l * T] >> 21) & 0x3FFu, theirs = r->t[l];
             if (mine != theirs) {
                 better = mine < theirs;
                 break;
@@ -397,7 +462,7 @@ __device__ void record_solution(const BtLaunch& P, const ThreadItem& s, const ui
         }
     }
     if (better) {
-        for (uint32_t l = 0; l < s.n; ++l) r->t[l] = static_cast<uint16_t>(stk[l * T + tid] >> 21);
+        for (uint32_t l = 0; l < s.n; ++l) r->t[l] = static_cast<uint16_t>((stk[l * T] >> 21) & 0x3FFu);
         r->has = 1;
     }
     __threadfence();
@@ -414,39 +479,45 @@ __device__ __forceinline__ void account(const BtLaunch& P, const ThreadItem& s)
     }
 }
 
-// Remaining candidates of level l (current level: from s.start; shallower
-// levels: after their placed transition), with `av` holding the availability
-// of level l's entry.
-template <int KW>
+// Remaining candidates of level l (current level: from s.start unless it is
+// known exhausted; shallower levels: after their placed transition, when the
+// `more` bit says some remain), with `av` holding level l's entry availability.
+template <int KW, bool SM, int T>
 __device__ __forceinline__ bool level_has_work(const BtLaunch& P, const ThreadItem& s, uint32_t l, const uint32_t* stk,
-                                               const uint64_t* av, const uint64_t* spill, uint32_t T, uint32_t tid,
-                                               uint32_t* start_out, uint32_t* spilled_out)
+                                               const uint64_t* av, const uint64_t* spill, uint32_t* start_out,
+                                               uint32_t* spilled_out)
 {
-    const LevelDesc d = load_desc(s.tb, s.desc_off, l);
+    const LevelDesc d = Tab<SM>::desc(s, l);
     uint32_t start, spilled;
+    bool maybe;
     if (l == s.L) {
         start = s.start;
         spilled = s.spilled;
+        maybe = !s.pop;
     } else {
-        const uint32_t e = stk[l * T + tid];
-        start = (e >> 21) + 1;
+        const uint32_t e = stk[l * T];
+        start = ((e >> 21) & 0x3FFu) + 1;
         spilled = (e >> 20) & 1u;
+        maybe = (e >> 31) != 0;
     }
-    uint64_t x[KW];
-    level_candidates<KW>(P, s, d, l, spilled != 0, stk, av, spill, T, tid, x);
-    uint32_t t;
     *start_out = start;
     *spilled_out = spilled;
-    return first_candidate<KW>(x, start, &t);
+    if (!maybe) return false;
+    uint64_t x[KW];
+    level_candidates<KW, SM, T>(P, s, d, l, spilled != 0, stk, av, spill, x);
+    uint32_t t;
+    bool more;
+    return first_candidate<KW>(x, start, &t, &more);
 }
 
+template <bool SM, int T>
 __device__ __forceinline__ void toggle_piece(const ThreadItem& s, uint32_t l, const uint32_t* stk, uint64_t* av,
-                                             uint32_t T, uint32_t tid, bool give_back)
+                                             bool give_back)
 {
-    const LevelDesc d = load_desc(s.tb, s.desc_off, l);
-    const uint32_t t = stk[l * T + tid] >> 21;
-    if (give_back) av[(d.aoff() + (t >> 6)) * T + tid] |= 0xFull << (t & 60u);
-    else av[(d.aoff() + (t >> 6)) * T + tid] &= ~(0xFull << (t & 60u));
+    const LevelDesc d = Tab<SM>::desc(s, l);
+    const uint32_t t = (stk[l * T] >> 21) & 0x3FFu;
+    if (give_back) av[(d.aoff() + (t >> 6)) * T] |= 0xFull << (t & 60u);
+    else av[(d.aoff() + (t >> 6)) * T] &= ~(0xFull << (t & 60u));
 }
 
 // Hands the remaining work of the thread's record to the next round: one
@@ -455,20 +526,19 @@ __device__ __forceinline__ void toggle_piece(const ThreadItem& s, uint32_t l, co
 // availability, and counts; pass 2 walks back down, writing records and taking
 // the pieces again, which leaves the state as it was.  Returns false when the
 // output queue is full (the thread then keeps the work).
-template <int KW>
-__device__ bool split_record(const BtLaunch& P, ThreadItem& s, uint32_t* stk, uint64_t* av, const uint64_t* spill,
-                             uint32_t T, uint32_t tid)
+template <int KW, bool SM, int T>
+__device__ bool split_record(const BtLaunch& P, ThreadItem& s, uint32_t* stk, uint64_t* av, const uint64_t* spill)
 {
     uint32_t cnt = 0, start, spilled;
     for (uint32_t l = s.L + 1; l-- > s.base;) {
-        if (l < s.L) toggle_piece(s, l, stk, av, T, tid, true);
-        cnt += level_has_work<KW>(P, s, l, stk, av, spill, T, tid, &start, &spilled);
+        if (l < s.L) toggle_piece<SM, T>(s, l, stk, av, true);
+        cnt += level_has_work<KW, SM, T>(P, s, l, stk, av, spill, &start, &spilled);
     }
     const unsigned long long slot = cnt ? atomicAdd(P.out_tail, (unsigned long long)cnt) : 0ull;
     const bool fits = slot + cnt <= P.out_capacity;
     unsigned long long k = slot;
     for (uint32_t l = s.base; l <= s.L; ++l) {
-        if (level_has_work<KW>(P, s, l, stk, av, spill, T, tid, &start, &spilled)) {
+        if (level_has_work<KW, SM, T>(P, s, l, stk, av, spill, &start, &spilled)) {
             if (fits) {
                 uint32_t* rec = P.out_rec + k * P.rec_words;
                 rec[0] = static_cast<uint32_t>(s.orig);
@@ -476,8 +546,8 @@ __device__ bool split_record(const BtLaunch& P, ThreadItem& s, uint32_t* stk, ui
                 rec[2] = l | (start << 16);
                 rec[3] = s.pz | (spilled << 16);
                 for (uint32_t j = 0; j < l; j += 2) {
-                    const uint32_t lo = stk[j * T + tid] >> 21;
-                    const uint32_t hi = j + 1 < l ? stk[(j + 1) * T + tid] >> 21 : 0u;
+                    const uint32_t lo = (stk[j * T] >> 21) & 0x3FFu;
+                    const uint32_t hi = j + 1 < l ? (stk[(j + 1) * T] >> 21) & 0x3FFu : 0u;
                     rec[4 + (j >> 1)] = lo | (hi << 16);
                 }
                 if (spilled)
@@ -491,18 +561,25 @@ __device__ bool split_record(const BtLaunch& P, ThreadItem& s, uint32_t* stk, ui
             }
             ++k;
         }
-        if (l < s.L) toggle_piece(s, l, stk, av, T, tid, false);
+        if (l < s.L) toggle_piece<SM, T>(s, l, stk, av, false);
     }
     return fits;
 }
 
-template <int KW, int kStepsPerFetch>
-__global__ void __launch_bounds__(256) dfs_kernel(BtLaunch P)
+template <int KW, bool SM, int T, int kStepsPerFetch>
+__global__ void __launch_bounds__(T) dfs_kernel(BtLaunch P)
 {
-    extern __shared__ __align__(16) uint32_t smem[];
-    const uint32_t T = blockDim.x, tid = threadIdx.x, lane = tid & 31;
-    uint32_t* stk = smem;
-    uint64_t* av = reinterpret_cast<uint64_t*>(smem + P.max_levels * T);
+    const uint32_t tid = threadIdx.x, lane = tid & 31;
+    if (SM) {
+        // stage the single puzzle's hot tables (words [0, smem_tab_words))
+        const uint4* src = reinterpret_cast<const uint4*>(P.tables + P.puzzle_offset[0]);
+        uint4* dst = reinterpret_cast<uint4*>(g_smem);
+        for (uint32_t i = tid; i < P.smem_tab_words / 4; i += T) dst[i] = __ldg(src + i);
+        __syncthreads();
+    }
+    // this thread's columns of the interleaved state
+    uint32_t* stk = g_smem + P.smem_tab_words + tid;
+    uint64_t* av = reinterpret_cast<uint64_t*>(g_smem + P.smem_tab_words + P.max_levels * T) + tid;
     uint64_t* spill = P.spill + (size_t)(blockIdx.x * T + tid) * P.max_levels * P.max_kw;
     ThreadItem s;
     s.active = false;
@@ -528,7 +605,7 @@ __global__ void __launch_bounds__(256) dfs_kernel(BtLaunch P)
                 if (my < P.n_in && !*(volatile int*)P.abort_flag) {
                     const uint32_t* rec = P.in_rec + my * P.rec_words;
                     if (!((rec[3] >> 17) & 1u)) {
-                        load_record(P, s, rec, stk, av, spill, T, tid);
+                        load_record<SM, T>(P, s, rec, stk, av, spill);
                         if (P.stop_at_first && s.orig > *(volatile unsigned long long*)&P.first_item[s.pz])
                             s.active = false;  // a lower subtree of this puzzle holds a solution
                     }
@@ -545,15 +622,19 @@ __global__ void __launch_bounds__(256) dfs_kernel(BtLaunch P)
         }
         if (!__any_sync(kFull, alive)) break;
 
-        // ---- DFS steps ----
-        for (int step = 0; step < kStepsPerFetch && s.active; ++step) {
-            bool solved = false;
-            if (dfs_step<KW>(P, s, stk, av, spill, T, tid, &solved)) {
-                if (solved) record_solution(P, s, stk, T, tid);
-                continue;
+        // ---- DFS steps: a warp-uniform trip count, lanes without work idle,
+        // every step ends reconverged ----
+        for (int step = 0; step < kStepsPerFetch; ++step) {
+            if (s.active) {
+                bool solved = false;
+                if (dfs_step<KW, SM, T>(P, s, stk, av, spill, &solved)) {
+                    if (solved) record_solution<T>(P, s, stk);
+                } else {
+                    account(P, s);
+                    s.active = false;
+                }
             }
-            account(P, s);
-            s.active = false;
+            __syncwarp();
         }
         if (!s.active) continue;
         s.steps += kStepsPerFetch;
@@ -561,7 +642,7 @@ __global__ void __launch_bounds__(256) dfs_kernel(BtLaunch P)
 
         // ---- once the queue is empty, hand work back for the next round ----
         if (drained && P.item_budget && s.steps >= P.item_budget) {
-            if (split_record<KW>(P, s, stk, av, spill, T, tid)) {
+            if (split_record<KW, SM, T>(P, s, stk, av, spill)) {
                 account(P, s);
                 s.active = false;
                 alive = false;
@@ -637,21 +718,36 @@ __global__ void record_prefix(const uint32_t* __restrict__ rec, uint32_t rec_wor
     for (uint32_t l = threadIdx.x; l < len; l += blockDim.x) out[l] = static_cast<uint16_t>(rec_t(r, l));
 }
 
-template <int KW>
-const void* dfs_symbol() { return reinterpret_cast<const void*>(&dfs_kernel<KW, 32>); }
+template <int KW, int T>
+const void* dfs_symbol(bool sm)
+{
+    return sm ? reinterpret_cast<const void*>(&dfs_kernel<KW, true, T, 32>)
+              : reinterpret_cast<const void*>(&dfs_kernel<KW, false, T, 32>);
+}
 
-const void* dfs_symbol_for(uint32_t max_kw)
+template <int T>
+const void* dfs_symbol_for_t(uint32_t max_kw, bool sm)
 {
     switch (max_kw) {
-        case 1: return dfs_symbol<1>();
-        case 2: return dfs_symbol<2>();
-        case 3: return dfs_symbol<3>();
-        case 4: return dfs_symbol<4>();
-        case 5: return dfs_symbol<5>();
-        case 6: return dfs_symbol<6>();
-        case 7: return dfs_symbol<7>();
-        case 8: return dfs_symbol<8>();
-        default: return max_kw <= 16 ? dfs_symbol<16>() : nullptr;
+        case 1: return dfs_symbol<1, T>(sm);
+        case 2: return dfs_symbol<2, T>(sm);
+        case 3: return dfs_symbol<3, T>(sm);
+        case 4: return dfs_symbol<4, T>(sm);
+        case 5: return dfs_symbol<5, T>(sm);
+        case 6: return dfs_symbol<6, T>(sm);
+        case 7: return dfs_symbol<7, T>(sm);
+        case 8: return dfs_symbol<8, T>(sm);
+        default: return max_kw <= 16 ? dfs_symbol<16, T>(sm) : nullptr;
+    }
+}
+
+const void* dfs_symbol_for(uint32_t max_kw, bool sm, uint32_t threads)
+{
+    switch (threads) {
+        case 64: return dfs_symbol_for_t<64>(max_kw, sm);
+        case 128: return dfs_symbol_for_t<128>(max_kw, sm);
+        case 256: return dfs_symbol_for_t<256>(max_kw, sm);
+        default: return nullptr;
     }
 }
 
@@ -687,20 +783,24 @@ cudaError_t launch_scan(const uint32_t* counts, uint64_t n, uint64_t* offsets, u
 
 uint64_t scan_block_sum_words(uint64_t n) { return (n + kScanBlock - 1) / kScanBlock + 1; }
 
-size_t dfs_smem_bytes(uint32_t max_levels, uint32_t max_avail_words, uint32_t threads)
+size_t dfs_smem_bytes(uint32_t max_levels, uint32_t max_avail_words, uint32_t threads, uint32_t tab_words)
 {
-    return (static_cast<size_t>(max_levels) * sizeof(uint32_t) + static_cast<size_t>(max_avail_words) * 8) * threads;
+    return static_cast<size_t>(tab_words) * sizeof(uint32_t) +
+           (static_cast<size_t>(max_levels) * sizeof(uint32_t) + static_cast<size_t>(max_avail_words) * 8) * threads;
 }
 
 uint32_t record_words(uint32_t max_levels, uint32_t max_kw) { return 4 + (max_levels + 1) / 2 + 2 * max_kw; }
 
-const void* dfs_kernel_symbol(uint32_t max_kw) { return dfs_symbol_for(max_kw); }
+const void* dfs_kernel_symbol(uint32_t max_kw, bool smem_tables, uint32_t threads)
+{
+    return dfs_symbol_for(max_kw, smem_tables, threads);
+}
 
 cudaError_t launch_dfs(const BtLaunch& P, uint32_t blocks, uint32_t threads, cudaStream_t stream)
 {
-    const void* fn = dfs_symbol_for(P.max_kw);
+    const void* fn = dfs_symbol_for(P.max_kw, P.smem_tab_words != 0, threads);
     if (!fn) return cudaErrorInvalidValue;
-    const size_t smem = dfs_smem_bytes(P.max_levels, P.max_avail_words, threads);
+    const size_t smem = dfs_smem_bytes(P.max_levels, P.max_avail_words, threads, P.smem_tab_words);
     void* args[] = {const_cast<BtLaunch*>(&P)};
     return cudaLaunchKernel(fn, dim3(blocks), dim3(threads), args, smem, stream);
 }

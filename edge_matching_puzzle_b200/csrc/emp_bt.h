@@ -32,6 +32,7 @@ struct BtLaunch {
     uint32_t max_avail_words = 0;             // max 64-bit availability words (three kinds)
     uint32_t max_kw = 0;                      // max 64-bit words of one kind
     uint64_t* spill = nullptr;                // [threads][max_levels][max_kw] remaining sets
+    uint32_t smem_tab_words = 0;              // > 0: single puzzle, hot tables staged in shared memory
     // work records of this round and of the next one
     const uint32_t* in_rec = nullptr;
     uint64_t n_in = 0;
@@ -60,7 +61,7 @@ cudaError_t launch_expand(const BtLaunch& P, const uint16_t* parents, const uint
 cudaError_t launch_scan(const uint32_t* counts, uint64_t n, uint64_t* offsets, uint64_t* block_sums,
                         uint64_t* grand_total, cudaStream_t stream);
 uint64_t scan_block_sum_words(uint64_t n);
-size_t dfs_smem_bytes(uint32_t max_levels, uint32_t max_avail_words, uint32_t threads);
+size_t dfs_smem_bytes(uint32_t max_levels, uint32_t max_avail_words, uint32_t threads, uint32_t tab_words);
 uint32_t record_words(uint32_t max_levels, uint32_t max_kw);
 cudaError_t launch_dfs(const BtLaunch& P, uint32_t blocks, uint32_t threads, cudaStream_t stream);
 cudaError_t launch_bt_reset(const BtLaunch& P, uint32_t n_puzzles, cudaStream_t stream);
@@ -69,6 +70,6 @@ cudaError_t launch_make_records(const uint16_t* prefixes, const uint32_t* prefix
                                 cudaStream_t stream);
 cudaError_t launch_record_prefix(const uint32_t* rec, uint32_t rec_words, uint64_t i, uint16_t* out,
                                  cudaStream_t stream);
-const void* dfs_kernel_symbol(uint32_t max_kw);
+const void* dfs_kernel_symbol(uint32_t max_kw, bool smem_tables, uint32_t threads);
 
 }  // namespace emp

@@ -32,18 +32,23 @@ __device__ __forceinline__ uint64_t ldg64(const uint32_t* p)
 
 struct LevelDesc {
     uint32_t d0, d1, d2, d3, d4, d5, d6, d7;
-    __device__ __forceinline__ uint32_t kind() const { return d0 & 3u; }
-    __device__ __forceinline__ uint32_t nplaced() const { return (d0 >> 2) & 7u; }
-    __device__ __forceinline__ uint32_t kw() const { return (d0 >> 8) & 0xFFu; }
+    __device__ __forceinline__ uint32_t kw() const { return d0 & 0xFFu; }
+    __device__ __forceinline__ uint32_t kind() const { return (d0 >> 8) & 3u; }
+    __device__ __forceinline__ uint32_t nextra() const { return (d0 >> 13) & 7u; }
     __device__ __forceinline__ uint32_t aoff() const { return d0 >> 16; }
-    __device__ __forceinline__ uint32_t arity() const { return d1 & 3u; }
-    __device__ __forceinline__ uint32_t side_a() const { return (d1 >> 2) & 3u; }
-    __device__ __forceinline__ uint32_t side_b() const { return (d1 >> 4) & 3u; }
-    __device__ __forceinline__ uint32_t level_a() const { return (d1 >> 8) & 0xFFu; }
-    __device__ __forceinline__ uint32_t level_b() const { return (d1 >> 16) & 0xFFu; }
-    __device__ __forceinline__ uint32_t nextra() const { return (d1 >> 24) & 3u; }
-    __device__ __forceinline__ uint32_t extra_side(uint32_t j) const { return (d3 >> (2 * j)) & 3u; }
-    __device__ __forceinline__ uint32_t extra_level(uint32_t j) const { return (d3 >> (8 + 8 * j)) & 0xFFu; }
+    __device__ __forceinline__ uint32_t level_a() const { return d1 & 0xFFu; }
+    __device__ __forceinline__ uint32_t level_b() const { return (d1 >> 8) & 0xFFu; }
+    __device__ __forceinline__ uint32_t shift_a() const { return (d1 >> 16) & 0xFFu; }
+    __device__ __forceinline__ uint32_t shift_b() const { return d1 >> 24; }
+    __device__ __forceinline__ uint32_t stride_a() const { return d3 & 0xFFFFu; }
+    __device__ __forceinline__ uint32_t stride_b() const { return d3 >> 16; }
+    __device__ __forceinline__ uint32_t extra_side(uint32_t j) const { return (d7 >> (2 * j)) & 3u; }
+    __device__ __forceinline__ uint32_t extra_level(uint32_t j) const { return (d7 >> (8 + 8 * j)) & 0xFFu; }
+    // pair-table row of this level given the stack words of neighbours A and B
+    __device__ __forceinline__ uint32_t row(uint32_t ea, uint32_t eb) const
+    {
+        return d2 + ((ea >> shift_a()) & 31u) * stride_a() + ((eb >> shift_b()) & 31u) * stride_b();
+    }
 };
 
 __device__ __forceinline__ LevelDesc load_desc(const uint32_t* tb, uint32_t desc_off, uint32_t L)

@@ -264,9 +264,6 @@ void build_device_tables(const PuzzleModel& m, const std::vector<LevelPlan>& pla
                 }
             }
         }
-        align(b, 4);
-        t.side_off[k] = static_cast<uint32_t>(b.size());
-        for (uint64_t v : side[k]) push64(b, v);
     }
     // pair tables, one per distinct (kind, base, paired sides) class
     align(b, 4);
@@ -339,6 +336,12 @@ void build_device_tables(const PuzzleModel& m, const std::vector<LevelPlan>& pla
             b.push_back(v);
         }
     }
+    // side masks: only read for the third and fourth placed neighbour of a level
+    for (uint32_t k = 0; k < 3; ++k) {
+        align(b, 4);
+        t.side_off[k] = static_cast<uint32_t>(b.size());
+        for (uint64_t v : side[k]) push64(b, v);
+    }
     for (uint32_t k = 0; k < 3; ++k) {
         align(b, 2);
         t.extra_off[k] = static_cast<uint32_t>(b.size());
@@ -373,18 +376,23 @@ void build_device_tables(const PuzzleModel& m, const std::vector<LevelPlan>& pla
         const LevelPlan& lp = plan[L];
         uint32_t* d = &b[t.desc_off + 8 * L];
         const uint32_t k = lp.kind;
-        d[0] = k | (lp.nplaced << 2) | (t.kw[k] << 8) | (t.aoff[k] << 16);
         const uint32_t arity = std::min<uint32_t>(lp.nplaced, 2);
-        d[1] = arity | ((arity > 0 ? lp.side[0] : 0u) << 2) | ((arity > 1 ? lp.side[1] : 0u) << 4) |
-               ((arity > 0 ? lp.nb_level[0] : 0u) << 8) | ((arity > 1 ? lp.nb_level[1] : 0u) << 16) |
-               ((lp.nplaced - arity) << 24);
+        const uint32_t nextra = lp.nplaced - arity;
+        // facing colour of the neighbour at side s sits at bits 5*((s+2)&3) of its stack word
+        const uint32_t shift_a = arity > 0 ? 5 * ((lp.side[0] + 2u) & 3u) : 0u;
+        const uint32_t shift_b = arity > 1 ? 5 * ((lp.side[1] + 2u) & 3u) : 0u;
+        const uint32_t stride_b = arity > 1 ? 2 * t.kw[k] : 0u;
+        const uint32_t stride_a = arity > 1 ? 2 * t.kw[k] * t.ncol : (arity > 0 ? 2 * t.kw[k] : 0u);
+        d[0] = t.kw[k] | (k << 8) | (nextra << 13) | (t.aoff[k] << 16);
+        d[1] = (arity > 0 ? lp.nb_level[0] : 0u) | ((arity > 1 ? lp.nb_level[1] : 0u) << 8) | (shift_a << 16) |
+               (shift_b << 24);
         d[2] = level_pair[L];
-        d[3] = (lp.nplaced > 2 ? lp.side[2] : 0u) | ((lp.nplaced > 3 ? lp.side[3] : 0u) << 2) |
-               ((lp.nplaced > 2 ? lp.nb_level[2] : 0u) << 8) | ((lp.nplaced > 3 ? lp.nb_level[3] : 0u) << 16);
+        d[3] = stride_a | (stride_b << 16);
         d[4] = t.side_off[k];
         d[5] = t.tinfo_off[k];
         d[6] = t.extra_off[k];
-        d[7] = lp.position;
+        d[7] = (nextra > 0 ? lp.side[2] : 0u) | ((nextra > 1 ? lp.side[3] : 0u) << 2) |
+               ((nextra > 0 ? lp.nb_level[2] : 0u) << 8) | ((nextra > 1 ? lp.nb_level[3] : 0u) << 16);
     }
     b[0] = 0x454D5032u;  // "EMP2"
     b[1] = t.n;
@@ -404,6 +412,7 @@ void build_device_tables(const PuzzleModel& m, const std::vector<LevelPlan>& pla
     b[23] = m.height;
     b[24] = static_cast<uint32_t>(b.size());
     b[25] = t.max_kw;
+    b[26] = t.side_off[0];  // words [0, side[0]) are what a kernel may stage in shared memory
 }
 
 namespace {

@@ -83,14 +83,19 @@ struct LevelPlan {
 //   6..8 aoff[k] (64-bit word offset of kind k in the availability array),
 //   9 avail words (64-bit), 10..12 side[k], 13 pair section, 14 desc,
 //   15..17 tinfo[k], 18..20 extra[k], 21 initial availability, 22 width,
-//   23 height, 24 blob words, 25 max kw
-// desc (8 words per level):
-//   d0 kind | nplaced<<2 | kw<<8 | aoff<<16
-//   d1 pair arity | sideA<<2 | sideB<<4 | levelA<<8 | levelB<<16 | nextra<<24
-//   d2 pair table (word offset): arity 2 [cA][cB][kw], 1 [cA][kw], 0 [kw];
+//   23 height, 24 blob words, 25 max kw, 26 words of the hot prefix
+// sections in order: header, pair tables, desc, tinfo, side, extra, initial
+// availability; the hot prefix [0, side[0]) is what the DFS reads at every step
+// desc (8 words per level; the first two placed neighbours A and B index the
+// level's pair table, further placed neighbours AND their side masks):
+//   d0 kw | kind<<8 | nextra<<13 | aoff<<16
+//   d1 levelA | levelB<<8 | shiftA<<16 | shiftB<<24 (bit offset of the
+//      neighbour's facing colour in its stack word)
+//   d2 pair table (word offset): rows [cA][cB][kw] (2 placed), [cA][kw] (1), [kw] (0);
 //      entries = frame-side masks & allowed orientations & placed-side masks
-//   d3 extra placed sides: side3 | side4<<2 | level3<<8 | level4<<16
-//   d4 side[kind], d5 tinfo[kind], d6 extra[kind], d7 position
+//   d3 strideA | strideB<<16 (words per colour step of A and B; 0 when absent)
+//   d4 side[kind], d5 tinfo[kind], d6 extra[kind],
+//   d7 extra placed sides: side3 | side4<<2 | level3<<8 | level4<<16
 // side[k]: 64-bit [side][colour][kw[k]] masks (colour ncol-1 = frame)
 // tinfo[k]: per transition t, colours of the oriented piece (5 bits per side)
 //           | has_extra<<20 (its identical mask clears other candidates)

@@ -54,7 +54,8 @@ class BtConfig(ctypes.Structure):
         ("split_budget", ctypes.c_uint32),
         ("sample_stride", ctypes.c_uint32),
         ("sample_first", ctypes.c_uint32),
-        ("reserved", ctypes.c_uint32 * 4),
+        ("table_placement", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32 * 3),
     ]
 
 

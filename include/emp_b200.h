@@ -98,7 +98,7 @@ emp_status emp_puzzle_export_tables(emp_puzzle puzzle, uint32_t *out, uint64_t c
 
 typedef struct emp_bt_config {
     uint32_t split_depth;        /* levels expanded before subtrees go to threads; 0 = auto */
-    uint32_t threads_per_block;  /* 0 = auto (autotuner cache or default) */
+    uint32_t threads_per_block;  /* 64, 128 or 256; 0 = the size with the most resident warps */
     uint32_t blocks_per_sm;      /* 0 = as many as fit */
     uint32_t stop_at_first;      /* 1: stop once the reference's first solution is known */
     uint64_t reserved_budget;    /* unused, keep 0 */
@@ -111,7 +111,9 @@ typedef struct emp_bt_config {
     uint32_t sample_stride;      /* emp_bt_count[_batch]: count only subtrees sample_first,
                                     sample_first+sample_stride, ...; 0 = all subtrees */
     uint32_t sample_first;
-    uint32_t reserved[4];
+    uint32_t table_placement;    /* 0 = auto (shared memory for a single puzzle), 1 = global memory,
+                                    2 = shared memory (single puzzle only) */
+    uint32_t reserved[3];
 } emp_bt_config;
 
 typedef struct emp_bt_result {

@@ -72,7 +72,26 @@ def test_random_small_puzzles(seed):
         pz = generate(w, h, rng.randint(1, 3), rng.randint(2, 5), rng.randint(0, 1 << 30))
         if OraclePuzzle(w, h, pz.colors).estimate(2000) < 3e6:
             break
-    _check(pz, depths=(1, min(5, w * h - 1), w * h - 1), split_budget=rng.choice([0, 256]))
+    _check(pz, depths=(1, min(5, w * h - 1), w * h - 1), split_budget=rng.choice([0, 256]),
+           table_placement=seed % 2)  # shared-memory tables and global-memory tables
+
+
+def test_batch_of_small_puzzles_one_launch():
+    """Many small puzzles in one plan (tables read from global memory), per-puzzle parity."""
+    rng = random.Random(77)
+    puzzles = []
+    while len(puzzles) < 24:
+        n = rng.randint(4, 5)
+        pz = generate(n, n, rng.randint(2, 3), rng.randint(3, 5), rng.randint(0, 1 << 30))
+        if OraclePuzzle(n, n, pz.colors).estimate(1000) < 1e6:
+            puzzles.append(pz)
+    handles = [native.NativePuzzle(p.width, p.height, p.colors) for p in puzzles]
+    res = native.bt_count_batch(handles, split_depth=3, split_budget=128)
+    for pz, r in zip(puzzles, res):
+        want, _ = OraclePuzzle(pz.width, pz.height, pz.colors).run()
+        assert (r.nodes, r.solutions) == (want.nodes, want.solutions)
+        if want.solutions:
+            assert list(r.first_solution)[: pz.nb_pieces] == list(want.first_board)[: pz.nb_pieces]
 
 
 def test_quirky_identical_masks_present():
@@ -91,7 +110,8 @@ def test_8x8_subtree_parity_sample():  # noqa: D103
     assert npz.info().identical_masks_with_extra > 0
     op = OraclePuzzle(8, 8, pz.colors)
     depth = 18
-    plan = native.BtPlan([npz], split_depth=depth, keep_subtree_counts=1, split_budget=512, timeout_ms=60000)
+    plan = native.BtPlan([npz], split_depth=depth, keep_subtree_counts=1, split_budget=512, timeout_ms=60000,
+                         table_placement=1)
     total = plan.subtrees()
     count, _, _, _ = op.expand(depth)
     assert total == count

@@ -76,23 +76,38 @@ def _u64(blob, off, count):
     return [blob[off + 2 * i] | (blob[off + 2 * i + 1] << 32) for i in range(count)]
 
 
-def _candidates_from_tables(blob, h, level, neighbour_colours):
+def _candidates_from_tables(blob, h, level, neighbour_colours, order, w):
     """Decodes a level descriptor and returns (kind, candidate bits, placed sides):
-    pair-table row for the first two placed sides & side masks of the others."""
+    pair-table row for the first two placed neighbours & side masks of the others."""
     d = blob[h["desc"] + 8 * level: h["desc"] + 8 * level + 8]
-    kind, nplaced, kw = d[0] & 3, (d[0] >> 2) & 7, (d[0] >> 8) & 0xFF
-    arity = d[1] & 3
-    sides = [(d[1] >> 2) & 3, (d[1] >> 4) & 3][:arity] + [(d[3] >> (2 * j)) & 3 for j in range(nplaced - arity)]
+    kind, kw, nextra = (d[0] >> 8) & 3, d[0] & 0xFF, (d[0] >> 13) & 7
+    pos = order[level]
+
+    def side_of(nb_level):  # side of this position facing the neighbour placed at nb_level
+        q = order[nb_level]
+        return {pos - w: 0, pos + 1: 1, pos + w: 2, pos - 1: 3}[q]
+
+    lev_a, lev_b = d[1] & 0xFF, (d[1] >> 8) & 0xFF
+    stride_a, stride_b = d[3] & 0xFFFF, d[3] >> 16
+    sides = []
     row = d[2]
-    if arity == 1:
-        row += neighbour_colours[sides[0]] * kw * 2
-    elif arity == 2:
-        row += (neighbour_colours[sides[0]] * h["ncol"] + neighbour_colours[sides[1]]) * kw * 2
+    if stride_a:
+        sa = side_of(lev_a)
+        sides.append(sa)
+        assert (d[1] >> 16) & 0xFF == 5 * ((sa + 2) % 4)
+        row += neighbour_colours[sa] * stride_a
+    if stride_b:
+        sb = side_of(lev_b)
+        sides.append(sb)
+        assert d[1] >> 24 == 5 * ((sb + 2) % 4)
+        row += neighbour_colours[sb] * stride_b
     words = _u64(blob, row, kw)
-    for sd in sides[arity:]:
+    for j in range(nextra):
+        sd = (d[7] >> (2 * j)) & 3
+        sides.append(sd)
         off = d[4] + (sd * h["ncol"] + neighbour_colours[sd]) * kw * 2
         words = [a & b for a, b in zip(words, _u64(blob, off, kw))]
-    return kind, sum(w << (64 * i) for i, w in enumerate(words)), sides
+    return kind, sum(v << (64 * i) for i, v in enumerate(words)), sides
 
 
 @pytest.mark.parametrize("seed", [0, 1, 2, 3])
@@ -117,7 +132,7 @@ def test_side_masks_equal_reference_table(shape, seed, order_name):
         frame = [y == 0, x == w - 1, y == h - 1, x == 0]
         for _ in range(12):
             nb = {s: rng.choice(colours) for s in range(4)}
-            kind, got, placed = _candidates_from_tables(blob, hd, level, nb)
+            kind, got, placed = _candidates_from_tables(blob, hd, level, nb, order, w)
             code = 0
             for s in range(4):
                 slot = (s + 2) % 4
