@@ -1,0 +1,565 @@
+// Glutton max search for sm_100a.
+//
+// The method is the reference's CUDA_glutton_max kernel
+// (include/CUDA_glutton_max.h:1522-1637): at every level
+//   1. remove_invalid_transitions (:745-954): drop every candidate (position,
+//      piece, orientation) whose trial placement empties a free position or
+//      leaves an available piece with nowhere to go, until nothing changes;
+//   2. get_best_candidate (:1010-1301): score every remaining candidate by its
+//      trial (total remaining bits over positions and pieces, then
+//      (max << 16) + min), keep the first maximum in (info, word, bit) order,
+//      the last candidate at the last level;
+//   3. apply_best_candidate (:1306-1476): clear its bit, build the next level,
+//      push, apply the colour constraints of its sides;
+// popping when a level fails (CUDA_glutton_max_stack.h:437-522).
+//
+// B200 design: one 1024-thread block per search keeps the level in shared
+// memory together with per-level statistics -- nibble counts N[j][q] of piece
+// q at free position j, bit totals A[j], per-piece sums S[q] and, per piece,
+// the six smallest and six largest A[j]-N[j][q].  A trial then only scans the
+// (at most four) colour-constrained neighbour positions word by word; every
+// other position contributes A[j]-N[j][p] and the piece counts follow from
+// S[q]-N[i][q] minus what the neighbours lost.  This gives the reference's
+// (valid, total, min, max) exactly at a fraction of its cost.  Step 1 runs as
+// Jacobi passes (all candidates against the same level, then all removals):
+// validity only gets harder as bits disappear, so the passes reach the same
+// greatest fixpoint as the reference's in-place sweep, and they empty a
+// position exactly when the reference's sweep does.
+#include "emp_gm.h"
+
+#include <cuda_runtime.h>
+
+namespace emp {
+
+namespace {
+
+constexpr int kThreads = 1024;
+constexpr unsigned kFull = 0xFFFFFFFFu;
+
+struct GmSmem {
+    uint32_t X[256][32];       // infos of the current level
+    uint32_t inval[256][32];   // candidates found invalid in this pass
+    uint8_t N[256][256];       // N[j][q]: orientations of piece q left at info j
+    uint32_t lo[256][6];       // per piece q: six smallest (A[j]-N[j][q]) << 16 | j, ~0 empty
+    uint32_t hi[256][6];       // per piece q: six largest (A[j]-N[j][q]+1) << 16 | j, 0 empty
+    uint32_t cc[32][4][32];    // colour constraints
+    uint16_t A[256];           // bits of info j
+    uint16_t S[256];           // sum over j of N[j][q]
+    uint8_t pieces[256][4];
+    uint32_t position_index[256];
+    uint32_t info_index[256];
+    uint32_t avail[8];
+    unsigned long long warp_key[32];
+    uint32_t warp_order[32];
+    uint32_t warp_trials[32];
+    uint32_t sumA;
+    uint32_t any_invalid;
+    uint32_t any_empty;
+    uint32_t next_info;
+    uint32_t best_order;       // chosen candidate: info << 10 | word << 5 | bit; ~0 none
+    uint32_t level, new_level, pop_index, stop, apply_failed;
+};
+
+__device__ __forceinline__ uint32_t tri_base(uint32_t S, uint32_t L)
+{
+    return (S * (S + 1) - (S - L) * (S - L + 1)) / 2;
+}
+
+__device__ __forceinline__ uint64_t global_ns()
+{
+    uint64_t t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ uint32_t warp_sum(uint32_t v)
+{
+    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+    return v;
+}
+__device__ __forceinline__ uint32_t warp_min(uint32_t v)
+{
+    for (int o = 16; o; o >>= 1) v = min(v, __shfl_xor_sync(kFull, v, o));
+    return v;
+}
+__device__ __forceinline__ uint32_t warp_max(uint32_t v)
+{
+    for (int o = 16; o; o >>= 1) v = max(v, __shfl_xor_sync(kFull, v, o));
+    return v;
+}
+
+__device__ __forceinline__ bool piece_available(const GmSmem& sm, uint32_t q)
+{
+    return (sm.avail[q >> 5] >> (q & 31)) & 1u;
+}
+
+// Per-pass statistics of the current level (block-wide).
+__device__ void level_statistics(GmSmem& sm, uint32_t nb, uint32_t tid)
+{
+    const uint32_t lane = tid & 31, warp = tid >> 5;
+    for (uint32_t j = warp; j < nb; j += kThreads / 32) {
+        const uint32_t word = sm.X[j][lane];
+        uint32_t packed0 = 0, packed1 = 0;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            packed0 |= static_cast<uint32_t>(__popc((word >> (4 * k)) & 0xFu)) << (8 * k);
+            packed1 |= static_cast<uint32_t>(__popc((word >> (4 * (k + 4))) & 0xFu)) << (8 * k);
+        }
+        reinterpret_cast<uint32_t*>(sm.N[j])[2 * lane] = packed0;
+        reinterpret_cast<uint32_t*>(sm.N[j])[2 * lane + 1] = packed1;
+        const uint32_t a = warp_sum(__popc(word));
+        if (lane == 0) sm.A[j] = static_cast<uint16_t>(a);
+    }
+    __syncthreads();
+    if (tid < 256) {
+        // S[q] and the six smallest A[j]-N[j][q]
+        const uint32_t q = tid;
+        uint32_t s = 0;
+        uint32_t best[6] = {~0u, ~0u, ~0u, ~0u, ~0u, ~0u};
+        for (uint32_t j = 0; j < nb; ++j) {
+            const uint32_t n = sm.N[j][q];
+            s += n;
+            uint32_t v = ((sm.A[j] - n) << 16) | j;
+#pragma unroll
+            for (int k = 0; k < 6; ++k) {
+                const uint32_t lo = min(best[k], v), hi2 = max(best[k], v);
+                best[k] = lo;
+                v = hi2;
+            }
+        }
+        sm.S[q] = static_cast<uint16_t>(s);
+#pragma unroll
+        for (int k = 0; k < 6; ++k) sm.lo[q][k] = best[k];
+    } else if (tid < 512) {
+        // the six largest, stored as (A[j]-N[j][q]+1) << 16 | j so that 0 marks an empty slot
+        const uint32_t q = tid - 256;
+        uint32_t best[6] = {0, 0, 0, 0, 0, 0};
+        for (uint32_t j = 0; j < nb; ++j) {
+            uint32_t v = ((sm.A[j] - sm.N[j][q] + 1u) << 16) | j;
+#pragma unroll
+            for (int k = 0; k < 6; ++k) {
+                const uint32_t big = max(best[k], v), small = min(best[k], v);
+                best[k] = big;
+                v = small;
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < 6; ++k) sm.hi[q][k] = best[k];
+    } else if (tid < 544) {
+        uint32_t a = 0;
+        for (uint32_t j = tid - 512; j < nb; j += 32) a += sm.A[j];
+        a = warp_sum(a);
+        uint32_t empty = 0;
+        for (uint32_t j = tid - 512; j < nb; j += 32) empty |= sm.A[j] == 0;
+        empty = __any_sync(kFull, empty);
+        if (tid == 512) {
+            sm.sumA = a;
+            sm.any_empty = empty;
+        }
+    }
+    __syncthreads();
+}
+
+struct Trial {
+    bool valid;
+    uint32_t total, mn, mx;
+};
+
+// Trial placement of (info i, word wc, bit b) on the current level, warp-wide
+// (lane w owns word w, i.e. pieces 8w..8w+7).  Mirrors the lambdas of
+// remove_invalid_transitions and get_best_candidate.
+__device__ Trial trial(const GmSmem& sm, uint32_t nb, uint32_t i, uint32_t wc, uint32_t b, uint32_t width,
+                       uint32_t lane)
+{
+    Trial r{true, 0, ~0u, 0};
+    const uint32_t p = 8 * wc + b / 4, o = b & 3u;
+    const uint32_t pos = sm.position_index[i];
+    const uint32_t pm = lane == wc ? ~(0xFu << (4 * (b / 4))) : kFull;
+    const int off[4] = {-static_cast<int>(width), 1, static_cast<int>(width), -1};
+    uint32_t nj[4], ncnt[4];
+    uint32_t nn = 0;
+    // apply_color_constraints (CUDA_glutton_max.h:531-612)
+    for (uint32_t s = 0; s < 4; ++s) {
+        const uint32_t col = sm.pieces[p][(s + o) & 3u];
+        if (!col) continue;
+        const uint32_t npos = static_cast<uint32_t>(static_cast<int>(pos) + off[s]);
+        const uint32_t j = sm.info_index[npos];
+        if (j >= nb) continue;  // position not free
+        const uint32_t rw = sm.X[j][lane] & sm.cc[col - 1][s][lane] & pm;
+        const uint32_t pc = warp_sum(__popc(rw));
+        if (!pc) {
+            r.valid = false;
+            return r;
+        }
+        uint32_t packed = 0;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) packed |= static_cast<uint32_t>(__popc((rw >> (4 * k)) & 0xFu)) << (3 * k);
+        nj[nn] = j;
+        ncnt[nn] = packed;
+        ++nn;
+        r.total += pc;
+        r.mn = min(r.mn, pc);
+        r.mx = max(r.mx, pc);
+    }
+    // every other free position keeps X[j] without piece p (apply_simple_mask)
+    uint32_t sum_a = sm.sumA - sm.A[i];
+    uint32_t sum_n = sm.S[p] - sm.N[i][p];
+    for (uint32_t k = 0; k < nn; ++k) {
+        sum_a -= sm.A[nj[k]];
+        sum_n -= sm.N[nj[k]][p];
+    }
+    r.total += sum_a - sum_n;
+    auto excluded = [&](uint32_t j) {
+        bool e = j == i;
+        for (uint32_t k = 0; k < nn; ++k) e |= j == nj[k];
+        return e;
+    };
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+        const uint32_t e = sm.lo[p][k];
+        if (e == ~0u) break;
+        if (!excluded(e & 0xFFFFu)) {
+            const uint32_t v = e >> 16;
+            if (v == 0) {
+                r.valid = false;
+                return r;
+            }
+            r.mn = min(r.mn, v);
+            break;
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+        const uint32_t e = sm.hi[p][k];
+        if (e == 0u) break;
+        if (!excluded(e & 0xFFFFu)) {
+            r.mx = max(r.mx, (e >> 16) - 1u);
+            break;
+        }
+    }
+    // pieces: every available piece other than p needs a place left
+    uint32_t psum = 0, pmin = ~0u, pmax = 0;
+    bool bad = false;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const uint32_t q = 8 * lane + k;
+        if (q == p || !piece_available(sm, q)) continue;
+        uint32_t c = static_cast<uint32_t>(sm.S[q]) - sm.N[i][q];
+        for (uint32_t kk = 0; kk < nn; ++kk) c -= sm.N[nj[kk]][q] - ((ncnt[kk] >> (3 * k)) & 7u);
+        bad |= c == 0;
+        psum += c;
+        pmin = min(pmin, c);
+        pmax = max(pmax, c);
+    }
+    if (__any_sync(kFull, bad)) {
+        r.valid = false;
+        return r;
+    }
+    r.total += warp_sum(psum);
+    r.mn = min(r.mn, warp_min(pmin));
+    r.mx = max(r.mx, warp_max(pmax));
+    return r;
+}
+
+__device__ void load_level(GmSmem& sm, const GmLaunch& P, uint32_t level, uint32_t tid)
+{
+    const uint32_t S = P.n, nb = S - level;
+    const uint32_t* src = P.infos + static_cast<size_t>(tri_base(S, level)) * 32;
+    for (uint32_t k = tid; k < nb * 32; k += kThreads) sm.X[k >> 5][k & 31] = src[k];
+}
+
+__device__ void store_level(const GmSmem& sm, const GmLaunch& P, uint32_t level, uint32_t tid)
+{
+    const uint32_t S = P.n, nb = S - level;
+    uint32_t* dst = P.infos + static_cast<size_t>(tri_base(S, level)) * 32;
+    for (uint32_t k = tid; k < nb * 32; k += kThreads) dst[k] = sm.X[k >> 5][k & 31];
+}
+
+// CUDA_glutton_max_stack::pop (thread 0); returns the restored info index.
+__device__ uint32_t pop_state(GmSmem& sm, GmState* st, uint32_t S)
+{
+    const uint32_t level = sm.level;
+    const uint32_t last = S - level;
+    const uint32_t info = sm.position_index[last];
+    const uint32_t played = st->played[level - 1];
+    const uint32_t pos = played & 0xFFu;
+    sm.level = level - 1;
+    const uint32_t piece = (played >> 8) & 0xFFu;
+    sm.avail[piece >> 5] |= 1u << (piece & 31);
+    sm.position_index[last] = pos;
+    const uint32_t pos2 = sm.position_index[info];
+    uint32_t t = sm.info_index[pos];
+    sm.info_index[pos] = sm.info_index[pos2];
+    sm.info_index[pos2] = t;
+    t = sm.position_index[info];
+    sm.position_index[info] = sm.position_index[last];
+    sm.position_index[last] = t;
+    st->pops++;
+    return info;
+}
+
+// CUDA_glutton_max_stack::push (thread 0).
+__device__ void push_state(GmSmem& sm, GmState* st, uint32_t S, uint32_t info, uint32_t pos, uint32_t piece, uint32_t o)
+{
+    const uint32_t level = sm.level;
+    st->played[level] = (o << 16) | (piece << 8) | pos;
+    sm.avail[piece >> 5] &= ~(1u << (piece & 31));
+    const uint32_t nl = level + 1;
+    sm.level = nl;
+    if (nl > st->max) {
+        for (uint32_t l = 0; l <= st->max && l < S; ++l) st->max_played[l] = st->played[l];
+        st->max = nl;
+    }
+    const uint32_t last = S - nl;
+    const uint32_t last_pos = sm.position_index[last];
+    sm.position_index[info] = info;
+    uint32_t t = sm.info_index[pos];
+    sm.info_index[pos] = sm.info_index[last_pos];
+    sm.info_index[last_pos] = t;
+    t = sm.position_index[info];
+    sm.position_index[info] = sm.position_index[last];
+    sm.position_index[last] = t;
+    st->pushes++;
+}
+
+__global__ void __launch_bounds__(kThreads, 1) gm_kernel(GmLaunch P)
+{
+    extern __shared__ __align__(16) unsigned char gm_raw[];
+    GmSmem& sm = *reinterpret_cast<GmSmem*>(gm_raw);
+    const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const uint32_t S = P.n;
+    GmState* st = P.state;
+    for (uint32_t k = tid; k < 256 * 4; k += kThreads) sm.pieces[k >> 2][k & 3] = P.pieces[k];
+    for (uint32_t k = tid; k < P.ncolours * 4 * 32; k += kThreads) (&sm.cc[0][0][0])[k] = P.cc[k];
+    for (uint32_t k = tid; k < 256; k += kThreads) {
+        sm.position_index[k] = st->position_index[k];
+        sm.info_index[k] = st->info_index[k];
+    }
+    if (tid < 8) sm.avail[tid] = st->avail[tid];
+    if (tid == 0) {
+        sm.level = st->level;
+        sm.new_level = st->new_level;
+        sm.pop_index = st->pop_index;
+        sm.stop = 0;
+    }
+    __syncthreads();
+    load_level(sm, P, sm.level, tid);
+    __syncthreads();
+    const uint64_t deadline = P.timeout_ns ? global_ns() + P.timeout_ns : 0;
+
+    for (;;) {
+        const uint32_t level = sm.level;
+        if (level >= S) break;  // full board (level == S) or exhausted (wrapped below 0)
+        if (tid == 0) {
+            if ((P.push_budget && st->pushes >= P.push_budget) || (deadline && global_ns() > deadline)) sm.stop = 1;
+        }
+        __syncthreads();
+        if (sm.stop) break;
+        const uint32_t nb = S - level;
+        // a popped level whose tried candidate was its last one pops again
+        if (!sm.new_level) {
+            const uint32_t any = __syncthreads_or(tid < 32 && sm.X[sm.pop_index][tid] != 0);
+            if (!any) {
+                __syncthreads();
+                if (tid == 0) {
+                    if (level == 0) sm.level = ~0u;
+                    else sm.pop_index = pop_state(sm, st, S);
+                    sm.new_level = 0;
+                }
+                __syncthreads();
+                if (sm.level < S) load_level(sm, P, sm.level, tid);
+                __syncthreads();
+                continue;
+            }
+        }
+        if (tid == 0) st->levels++;
+        // ---- validity fixpoint and scores ----
+        bool failed = false;
+        for (;;) {
+            level_statistics(sm, nb, tid);
+            if (sm.any_empty) {
+                failed = true;
+                break;
+            }
+            for (uint32_t k = tid; k < nb * 32; k += kThreads) sm.inval[k >> 5][k & 31] = 0;
+            if (tid == 0) {
+                sm.any_invalid = 0;
+                sm.next_info = 0;
+                st->passes++;
+            }
+            __syncthreads();
+            unsigned long long best_key = 0;
+            uint32_t best_order = ~0u, trials = 0;
+            const bool last_level = level == S - 1;
+            for (;;) {
+                uint32_t i = 0;
+                if (lane == 0) i = atomicAdd(&sm.next_info, 1u);
+                i = __shfl_sync(kFull, i, 0);
+                if (i >= nb) break;
+                for (uint32_t w = 0; w < 32; ++w) {
+                    uint32_t word = sm.X[i][w];
+                    while (word) {
+                        const uint32_t b = __ffs(word) - 1;
+                        word &= word - 1;
+                        ++trials;
+                        const Trial t = trial(sm, nb, i, w, b, P.width, lane);
+                        const uint32_t order = (i << 10) | (w << 5) | b;
+                        if (!t.valid) {
+                            if (lane == 0) {
+                                atomicOr(&sm.inval[i][w], 1u << b);
+                                sm.any_invalid = 1;
+                            }
+                            continue;
+                        }
+                        const unsigned long long key =
+                            (static_cast<unsigned long long>(t.total) << 32) | ((t.mx << 16) + t.mn);
+                        const bool better = best_order == ~0u ||
+                                            (last_level ? order > best_order
+                                                        : (key > best_key || (key == best_key && order < best_order)));
+                        if (better) {
+                            best_key = key;
+                            best_order = order;
+                        }
+                    }
+                }
+            }
+            if (lane == 0) {
+                sm.warp_key[warp] = best_key;
+                sm.warp_order[warp] = best_order;
+                sm.warp_trials[warp] = trials;
+            }
+            __syncthreads();
+            if (!sm.any_invalid) {
+                if (tid == 0) {
+                    unsigned long long k0 = 0;
+                    uint32_t o0 = ~0u;
+                    unsigned long long tr = 0;
+                    for (int w = 0; w < kThreads / 32; ++w) {
+                        tr += sm.warp_trials[w];
+                        const uint32_t o = sm.warp_order[w];
+                        if (o == ~0u) continue;
+                        const unsigned long long k = sm.warp_key[w];
+                        const bool better =
+                            o0 == ~0u || (last_level ? o > o0 : (k > k0 || (k == k0 && o < o0)));
+                        if (better) {
+                            k0 = k;
+                            o0 = o;
+                        }
+                    }
+                    sm.best_order = o0;
+                    st->trials += tr;
+                }
+                __syncthreads();
+                break;
+            }
+            if (tid == 0) {
+                unsigned long long tr = 0;
+                for (int w = 0; w < kThreads / 32; ++w) tr += sm.warp_trials[w];
+                st->trials += tr;
+            }
+            for (uint32_t k = tid; k < nb * 32; k += kThreads) sm.X[k >> 5][k & 31] &= ~sm.inval[k >> 5][k & 31];
+            __syncthreads();
+        }
+        if (failed || sm.best_order == ~0u) {
+            // remove_invalid_transitions failed or no candidate: pop
+            __syncthreads();
+            if (tid == 0) {
+                if (level == 0) sm.level = ~0u;
+                else sm.pop_index = pop_state(sm, st, S);
+                sm.new_level = 0;
+            }
+            __syncthreads();
+            if (sm.level < S) load_level(sm, P, sm.level, tid);
+            __syncthreads();
+            continue;
+        }
+        // ---- apply_best_candidate ----
+        const uint32_t bi = sm.best_order >> 10, bw = (sm.best_order >> 5) & 31u, bb = sm.best_order & 31u;
+        const uint32_t piece = 8 * bw + bb / 4, o = bb & 3u;
+        const uint32_t pos = sm.position_index[bi];
+        if (tid == 0) sm.X[bi][bw] &= ~(1u << bb);
+        __syncthreads();
+        store_level(sm, P, level, tid);  // the level keeps its remaining candidates for a later pop
+        const uint32_t pm_word = ~(0xFu << (4 * (bb / 4)));
+        // the next level moves the last info into the chosen slot; an empty
+        // result there stops the reference's apply before its push
+        const bool copy_last = bi < nb - 1 && level < S - 1;
+        const uint32_t last_any =
+            copy_last ? __syncthreads_or(tid < 32 && (sm.X[nb - 1][tid] & (tid == bw ? pm_word : kFull)) != 0) : 1u;
+        if (!last_any) {
+            if (tid == 0) sm.new_level = 1;
+            __syncthreads();
+            continue;
+        }
+        __syncthreads();
+        // next level in place: X[j] &= pm for j < nb-1, X[bi] = X[nb-1] & pm
+        for (uint32_t k = tid; k < (nb - 1) * 32; k += kThreads) {
+            const uint32_t j = k >> 5, w = k & 31;
+            const uint32_t m = w == bw ? pm_word : kFull;
+            if (j == bi) sm.X[j][w] = sm.X[nb - 1][w] & m;
+            else sm.X[j][w] &= m;
+        }
+        __syncthreads();
+        if (tid == 0) push_state(sm, st, S, bi, pos, piece, o);
+        __syncthreads();
+        // colour constraints of the placed piece on its free neighbours
+        if (warp == 0) {
+            const uint32_t nl = sm.level, nbn = S - nl;
+            const int off[4] = {-static_cast<int>(P.width), 1, static_cast<int>(P.width), -1};
+            bool invalid = false;
+            for (uint32_t s = 0; s < 4 && !invalid; ++s) {
+                const uint32_t col = sm.pieces[piece][(s + o) & 3u];
+                if (!col) continue;
+                const uint32_t npos = static_cast<uint32_t>(static_cast<int>(pos) + off[s]);
+                const uint32_t j = sm.info_index[npos];
+                if (j >= nbn) continue;
+                const uint32_t r = sm.X[j][lane] & sm.cc[col - 1][s][lane];
+                if (!__any_sync(kFull, r)) {
+                    invalid = true;
+                    break;
+                }
+                sm.X[j][lane] = r;
+            }
+            if (lane == 0) sm.apply_failed = invalid;
+        }
+        __syncthreads();
+        if (sm.apply_failed) {
+            __syncthreads();
+            if (tid == 0) pop_state(sm, st, S);
+            __syncthreads();
+            load_level(sm, P, sm.level, tid);
+        }
+        if (tid == 0) sm.new_level = 1;
+        __syncthreads();
+    }
+    // write the search state back
+    __syncthreads();
+    if (tid == 0) {
+        const uint32_t level = sm.level;
+        st->level = level;
+        st->new_level = sm.new_level;
+        st->pop_index = sm.pop_index;
+        st->status = level == S ? 0 : (level > S ? 2 : 1);
+    }
+    if (sm.level < S) store_level(sm, P, sm.level, tid);
+    for (uint32_t k = tid; k < 256; k += kThreads) {
+        st->position_index[k] = sm.position_index[k];
+        st->info_index[k] = sm.info_index[k];
+    }
+    if (tid < 8) st->avail[tid] = sm.avail[tid];
+}
+
+}  // namespace
+
+size_t gm_smem_bytes() { return sizeof(GmSmem); }
+
+cudaError_t launch_gm(const GmLaunch& P, cudaStream_t stream)
+{
+    const size_t smem = sizeof(GmSmem);
+    cudaError_t e = cudaFuncSetAttribute(gm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    if (e != cudaSuccess) return e;
+    gm_kernel<<<1, kThreads, smem, stream>>>(P);
+    return cudaGetLastError();
+}
+
+}  // namespace emp

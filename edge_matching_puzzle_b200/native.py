@@ -79,6 +79,28 @@ class BtResult(ctypes.Structure):
     ]
 
 
+class GmConfig(ctypes.Structure):
+    _fields_ = [("push_budget", ctypes.c_uint64), ("timeout_ms", ctypes.c_uint32), ("device", ctypes.c_int32),
+                ("reserved", ctypes.c_uint32 * 8)]
+
+
+class GmResult(ctypes.Structure):
+    _fields_ = [
+        ("status", ctypes.c_int32),
+        ("max_level", ctypes.c_uint32),
+        ("level", ctypes.c_uint32),
+        ("reserved0", ctypes.c_uint32),
+        ("best_board", ctypes.c_uint32 * 256),
+        ("final_board", ctypes.c_uint32 * 256),
+        ("trials", ctypes.c_uint64),
+        ("pushes", ctypes.c_uint64),
+        ("pops", ctypes.c_uint64),
+        ("passes", ctypes.c_uint64),
+        ("levels", ctypes.c_uint64),
+        ("kernel_ms", ctypes.c_double),
+    ]
+
+
 # name -> (restype, argtypes); every symbol declared in include/emp_b200.h
 SIGNATURES = {
     "emp_abi_version": (ctypes.c_uint32, []),
@@ -101,6 +123,7 @@ SIGNATURES = {
     "emp_bt_plan_subtree_counts": (ctypes.c_int32, [ctypes.c_void_p, u64p, u64p, ctypes.c_uint64]),
     "emp_bt_plan_subtree_prefix": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_uint64, u16p, ctypes.c_uint32]),
     "emp_bt_plan_destroy": (None, [ctypes.c_void_p]),
+    "emp_glutton_max": (ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(GmConfig), ctypes.POINTER(GmResult)]),
 }
 
 _lib = None
@@ -199,6 +222,16 @@ def bt_count_batch(puzzles: Sequence[NativePuzzle], **kw) -> List[BtResult]:
     cfg = bt_config(**kw)
     check(load().emp_bt_count_batch(arr, len(puzzles), ctypes.byref(cfg), res))
     return list(res)
+
+
+def glutton_max(puzzle: NativePuzzle, push_budget: int = 0, timeout_ms: int = 0, device: int = -1) -> GmResult:
+    cfg = GmConfig()
+    cfg.push_budget = push_budget
+    cfg.timeout_ms = timeout_ms
+    cfg.device = device
+    r = GmResult()
+    check(load().emp_glutton_max(puzzle.handle, ctypes.byref(cfg), ctypes.byref(r)))
+    return r
 
 
 class BtPlan:

@@ -166,6 +166,37 @@ emp_status emp_bt_plan_subtree_counts(emp_bt_plan plan, uint64_t *nodes, uint64_
 emp_status emp_bt_plan_subtree_prefix(emp_bt_plan plan, uint64_t index, uint16_t *prefix, uint32_t capacity);
 void emp_bt_plan_destroy(emp_bt_plan plan);
 
+/* ---------------- glutton max search (CUDA_glutton_max semantics) ---------------- */
+
+typedef struct emp_gm_config {
+    uint64_t push_budget;        /* stop after this many committed placements; 0 = none */
+    uint32_t timeout_ms;         /* stop after this long on the device; 0 = one hour */
+    int32_t device;              /* CUDA device ordinal; -1 = current device */
+    uint32_t reserved[8];
+} emp_gm_config;
+
+typedef struct emp_gm_result {
+    int32_t status;              /* 0 full board, 1 stopped by budget or timeout, 2 search exhausted
+                                    (the reference's "Empty stack") */
+    uint32_t max_level;          /* most pieces placed at once (the stack's m_max) */
+    uint32_t level;              /* pieces placed in the final stack */
+    uint32_t reserved0;
+    uint32_t best_board[256];    /* best partial board: per position y*w+x (piece id-1)<<2 | orientation,
+                                    0xFFFFFFFF empty */
+    uint32_t final_board[256];   /* final stack (the reference's "Situation with stack played info") */
+    uint64_t trials;             /* candidate trial evaluations (all validity passes) */
+    uint64_t pushes;             /* committed placements */
+    uint64_t pops;
+    uint64_t passes;             /* validity passes */
+    uint64_t levels;             /* levels evaluated */
+    double kernel_ms;
+} emp_gm_result;
+
+/* Greedy max-placement search of one puzzle, as launch_CUDA_glutton_max
+ * (src/CUDA_glutton_max.cu:38-108) runs it: the same level-by-level choice of
+ * the best candidate, the same backtracking, the same final board. */
+emp_status emp_glutton_max(emp_puzzle puzzle, const emp_gm_config *config, emp_gm_result *result);
+
 #ifdef __cplusplus
 }
 #endif

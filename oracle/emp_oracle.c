@@ -1039,7 +1039,7 @@ static void gm_apply(gm_state *g, uint32_t best)
     if (invalid) gm_pop(g);
 }
 
-int op_gm_run(op_puzzle *p, uint64_t budget, op_gm_result *out)
+int op_gm_run(op_puzzle *p, uint64_t budget, uint64_t push_budget, op_gm_result *out)
 {
     memset(out, 0, sizeof(*out));
     gm_state *g = (gm_state *)calloc(1, sizeof(gm_state));
@@ -1102,6 +1102,7 @@ int op_gm_run(op_puzzle *p, uint64_t budget, op_gm_result *out)
     uint32_t pop_index = 0;
     while (g->level < g->size) {
         if (g->stop) break;
+        if (push_budget && out->pushes >= push_budget) { g->stop = 1; break; }
         if (!new_level && !gm_any(gm_info(g, g->level, pop_index))) {
             if (g->level == 0) { g->level = 0xFFFFFFFFu; break; }
             pop_index = gm_pop(g);

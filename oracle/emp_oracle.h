@@ -121,8 +121,10 @@ typedef struct {
     uint64_t pushes, pops, levels_evaluated;
 } op_gm_result;
 
-/* Glutton max search (CUDA_glutton_max kernel semantics). */
-int op_gm_run(op_puzzle *p, uint64_t budget, op_gm_result *out);
+/* Glutton max search (CUDA_glutton_max kernel semantics).  budget: stop after
+ * that many placements (trials + pushes), push_budget: after that many
+ * pushes, checked at the top of each level (0: none). */
+int op_gm_run(op_puzzle *p, uint64_t budget, uint64_t push_budget, op_gm_result *out);
 
 #ifdef __cplusplus
 }

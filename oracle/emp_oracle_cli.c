@@ -75,7 +75,7 @@ int main(int argc, char **argv)
         free(log);
     } else if (!strcmp(argv[2], "glutton_max")) {
         op_gm_result r;
-        op_gm_run(p, budget, &r);
+        op_gm_run(p, budget, 0, &r);
         printf("Launch kernels\n");
         if (r.status == 2) {
             printf("Empty stack\n");

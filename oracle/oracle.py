@@ -88,7 +88,7 @@ def lib():
                                               ctypes.POINTER(u64), ctypes.POINTER(u64), ctypes.POINTER(u64)]
         L.op_bt_estimate.restype = ctypes.c_double
         L.op_bt_estimate.argtypes = [vp, ctypes.POINTER(u32), u32, u64, ctypes.POINTER(ctypes.c_double)]
-        L.op_gm_run.argtypes = [vp, u64, ctypes.POINTER(GmResult)]
+        L.op_gm_run.argtypes = [vp, u64, u64, ctypes.POINTER(GmResult)]
         _lib = L
     return _lib
 
@@ -191,7 +191,7 @@ class OraclePuzzle:
     def estimate(self, probes: int, seed: int = 1, order=None) -> float:
         return lib().op_bt_estimate(self._p, self._order(order), probes, seed, None)
 
-    def glutton(self, budget: int = 0) -> GmResult:
+    def glutton(self, budget: int = 0, push_budget: int = 0) -> GmResult:
         r = GmResult()
-        lib().op_gm_run(self._p, budget, ctypes.byref(r))
+        lib().op_gm_run(self._p, budget, push_budget, ctypes.byref(r))
         return r

@@ -1,0 +1,64 @@
+"""GPU parity of the glutton max search against the CPU oracle (restatement of
+include/CUDA_glutton_max.h, pinned on the reference's tests/CUDA_glutton_max_* boards).
+
+The search trajectory (every push and pop, the final and best boards) must be
+identical; the number of candidate trials is not compared, because the GPU runs the
+validity fixpoint as passes over a fixed level instead of the reference's in-place
+sweep (same fixpoint, different number of evaluations)."""
+from __future__ import annotations
+
+import random
+
+import pytest
+
+from edge_matching_puzzle_b200 import native
+from edge_matching_puzzle_b200.puzzle import Puzzle, board_string, generate
+from oracle.oracle import OraclePuzzle
+
+pytestmark = pytest.mark.gpu
+
+
+def _boards(pz, r):
+    cells = [-1] * pz.nb_pieces
+    for level in range(r.level if r.status == 0 else 0):
+        pi = r.played[level]
+        cells[pi & 0xFF] = (((pi >> 8) & 0xFF) << 2) | (pi >> 16)
+    best = [-1] * pz.nb_pieces
+    for level in range(r.max_level):
+        pi = r.max_played[level]
+        if pi != 0xFFFFFFFF:
+            best[pi & 0xFF] = (((pi >> 8) & 0xFF) << 2) | (pi >> 16)
+    return cells, best
+
+
+@pytest.mark.parametrize("name", ["3_3", "4_4", "5_5"])
+def test_reference_glutton_boards(reference_vectors, name):
+    pz = Puzzle.from_csv(reference_vectors["puzzles"][name])
+    r = native.glutton_max(native.NativePuzzle(pz.width, pz.height, pz.colors), timeout_ms=60000)
+    assert r.status == 0
+    assert board_string(pz.width, pz.height, list(r.final_board)) == reference_vectors["glutton_max"][name][-1]
+
+
+def _compare(pz, push_budget=0):
+    want = OraclePuzzle(pz.width, pz.height, pz.colors).glutton(push_budget=push_budget)
+    got = native.glutton_max(native.NativePuzzle(pz.width, pz.height, pz.colors), push_budget=push_budget,
+                             timeout_ms=60000)
+    assert (got.status, got.max_level, got.pushes, got.pops, got.levels) == \
+        (want.status, want.max_level, want.pushes, want.pops, want.levels_evaluated)
+    cells, best = _boards(pz, want)
+    if want.status == 0:
+        assert list(got.final_board)[: pz.nb_pieces] == [c & 0xFFFFFFFF for c in cells]
+    assert [c if c != 0xFFFFFFFF else -1 for c in list(got.best_board)[: pz.nb_pieces]] == best
+
+
+@pytest.mark.parametrize("seed", range(12))
+def test_random_puzzles_full_search(seed):
+    rng = random.Random(500 + seed)
+    w, h = rng.randint(3, 5), rng.randint(3, 5)
+    _compare(generate(w, h, rng.randint(2, 3), rng.randint(3, 6), seed))
+
+
+@pytest.mark.parametrize("seed,budget", [(0, 10), (1, 40), (2, 100)])
+def test_push_budget_trajectory(seed, budget):
+    """Bounded searches on larger puzzles stop at the same point with the same best board."""
+    _compare(generate(8, 8, 4, 8, seed), push_budget=budget)
