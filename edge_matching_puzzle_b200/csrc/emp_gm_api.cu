@@ -5,7 +5,10 @@
 
 #include <cuda_runtime.h>
 
+#include <chrono>
 #include <cstring>
+#include <mutex>
+#include <string>
 #include <vector>
 
 using emp::DeviceBuffer;
@@ -162,5 +165,133 @@ extern "C" emp_status emp_glutton_max(emp_puzzle puzzle, const emp_gm_config* co
     result->passes = st.passes;
     result->levels = st.levels;
     result->kernel_ms = ms;
+    return st.status == 1 ? EMP_INCOMPLETE : EMP_OK;
+}
+
+// ---------------------------------------------------------------------------
+// emp_glutton_max_noalloc: the same search with its device memory taken from a
+// fixed array compiled into this library instead of cudaMalloc.
+//
+// Layout of the array (byte offsets, each section 256-byte aligned):
+//   state   GmState
+//   pieces  256 x 4 colours
+//   cc      32 colours x 4 sides x 32 words
+//   infos   triangular level stack for 256 positions: 256*257/2 infos x 32 words
+// 4,232,448 bytes in all, enough for every puzzle the library accepts (at most
+// 256 pieces, colour ids up to 31).
+namespace {
+
+constexpr size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+constexpr uint32_t kNoAllocMaxPieces = 256;
+constexpr uint32_t kNoAllocMaxColours = 32;  // colour ids 1..31 plus the frame
+constexpr size_t kOffState = 0;
+constexpr size_t kOffPieces = align256(kOffState + sizeof(emp::GmState));
+constexpr size_t kOffCc = align256(kOffPieces + 256 * 4);
+constexpr size_t kOffInfos = align256(kOffCc + sizeof(uint32_t) * kNoAllocMaxColours * 4 * 32);
+constexpr size_t kNoAllocBytes =
+    align256(kOffInfos + sizeof(uint32_t) * 32 * (size_t(kNoAllocMaxPieces) * (kNoAllocMaxPieces + 1) / 2));
+static_assert(kNoAllocBytes == 4232448, "scratch size stated above");
+constexpr int kNoAllocMaxDevices = 64;
+
+std::mutex g_noalloc_mu;
+unsigned char* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+
+}  // namespace
+
+static __device__ __align__(256) unsigned char g_gm_scratch[kNoAllocBytes];
+
+extern "C" emp_status emp_glutton_max_noalloc(emp_puzzle puzzle, const emp_gm_config* config, emp_gm_result* result)
+{
+    emp::clear_error();
+    if (!puzzle || !result) return fail(EMP_ERR_INVALID, "emp_glutton_max_noalloc: null argument");
+    emp_gm_config cfg{};
+    cfg.device = -1;
+    if (config) cfg = *config;
+    const emp::PuzzleModel& m = puzzle->model;
+    if (m.n > kNoAllocMaxPieces)
+        return fail(EMP_ERR_UNSUPPORTED, "emp_glutton_max_noalloc: " + std::to_string(m.n) +
+                                             " pieces exceed the fixed scratch limit of " +
+                                             std::to_string(kNoAllocMaxPieces));
+    if (m.border_id > kNoAllocMaxColours)
+        return fail(EMP_ERR_UNSUPPORTED, "emp_glutton_max_noalloc: " + std::to_string(m.border_id) +
+                                             " colours exceed the fixed scratch limit of " +
+                                             std::to_string(kNoAllocMaxColours));
+    int dev = 0;
+    EMP_TRY(emp::select_device(cfg.device, &dev));
+    if (dev >= kNoAllocMaxDevices) return fail(EMP_ERR_UNSUPPORTED, "emp_glutton_max_noalloc: device ordinal above 63");
+    cudaDeviceProp prop;
+    CUDA_TRY(cudaGetDeviceProperties(&prop, dev));
+    if (emp::gm_smem_bytes() > static_cast<size_t>(prop.sharedMemPerBlockOptin))
+        return fail(EMP_ERR_UNSUPPORTED, "glutton max level state does not fit shared memory");
+
+    // One-time set-up per device, with that device current: look up the device
+    // address of the scratch array (this is what loads it onto the device).
+    unsigned char* base = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_noalloc_mu);
+        if (!g_noalloc_ptr[dev]) {
+            void* p = nullptr;
+            cudaError_t e = cudaGetSymbolAddress(&p, g_gm_scratch);
+            if (e != cudaSuccess) return emp::cuda_fail(e, "emp_glutton_max_noalloc: scratch address look-up");
+            g_noalloc_ptr[dev] = static_cast<unsigned char*>(p);
+        }
+        base = g_noalloc_ptr[dev];
+    }
+
+    const uint32_t S = m.n;
+    std::vector<uint8_t> pieces(256 * 4, 0);
+    for (uint32_t i = 0; i < m.n; ++i)
+        for (uint32_t s = 0; s < 4; ++s) pieces[4 * i + s] = m.colours[i][s];
+    const std::vector<uint32_t> cc = colour_constraints(m);
+    const std::vector<uint32_t> cap = initial_capability(m);
+    emp::GmState st;
+    std::memset(&st, 0, sizeof(st));
+    st.new_level = 1;
+    for (uint32_t i = 0; i < 256; ++i) {
+        st.position_index[i] = i < S ? i : 0xFFFFFFFFu;
+        st.info_index[i] = i < S ? i : 0xFFFFFFFFu;
+        st.played[i] = 0xFFFFFFFFu;
+        st.max_played[i] = 0xFFFFFFFFu;
+    }
+    for (uint32_t i = 0; i < m.n; ++i) st.avail[i >> 5] |= 1u << (i & 31);
+    // The array keeps whatever the previous call left.  Everything the kernel
+    // reads before writing is overwritten here: the whole state, all piece
+    // colours, the colour constraints of this puzzle's colours and the first
+    // level of the info stack.  Deeper levels are written by the kernel before
+    // they are read, exactly as with freshly allocated (uninitialised) memory.
+    CUDA_TRY(cudaMemcpy(base + kOffState, &st, sizeof(st), cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(base + kOffPieces, pieces.data(), pieces.size(), cudaMemcpyHostToDevice));
+    if (!cc.empty()) CUDA_TRY(cudaMemcpy(base + kOffCc, cc.data(), sizeof(uint32_t) * cc.size(), cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(base + kOffInfos, cap.data(), sizeof(uint32_t) * cap.size(), cudaMemcpyHostToDevice));
+    emp::GmLaunch P;
+    P.pieces = reinterpret_cast<const uint8_t*>(base + kOffPieces);
+    P.cc = reinterpret_cast<const uint32_t*>(base + kOffCc);
+    P.infos = reinterpret_cast<uint32_t*>(base + kOffInfos);
+    P.state = reinterpret_cast<emp::GmState*>(base + kOffState);
+    P.n = S;
+    P.width = m.width;
+    P.ncolours = m.border_id;
+    P.push_budget = cfg.push_budget;
+    const unsigned long long ms_limit = cfg.timeout_ms ? cfg.timeout_ms : 3600000ull;
+    P.timeout_ns = ms_limit * 1000000ull;
+    // no CUDA events (they are driver objects to create and destroy): the time
+    // reported is the host's wall time from launch to the result copy
+    const auto t0 = std::chrono::steady_clock::now();
+    cudaError_t le = emp::launch_gm(P, nullptr);
+    if (le != cudaSuccess) return emp::cuda_fail(le, "glutton max launch");
+    CUDA_TRY(cudaMemcpy(&st, base + kOffState, sizeof(st), cudaMemcpyDeviceToHost));
+    const auto t1 = std::chrono::steady_clock::now();
+    std::memset(result, 0, sizeof(*result));
+    result->status = st.status;
+    result->max_level = st.max;
+    result->level = st.level <= S ? st.level : 0;
+    board_from_played(m, st.max_played, st.max, result->best_board);
+    board_from_played(m, st.played, result->level, result->final_board);
+    result->trials = st.trials;
+    result->pushes = st.pushes;
+    result->pops = st.pops;
+    result->passes = st.passes;
+    result->levels = st.levels;
+    result->kernel_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
     return st.status == 1 ? EMP_INCOMPLETE : EMP_OK;
 }

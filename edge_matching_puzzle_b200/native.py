@@ -124,6 +124,7 @@ SIGNATURES = {
     "emp_bt_plan_subtree_prefix": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_uint64, u16p, ctypes.c_uint32]),
     "emp_bt_plan_destroy": (None, [ctypes.c_void_p]),
     "emp_glutton_max": (ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(GmConfig), ctypes.POINTER(GmResult)]),
+    "emp_glutton_max_noalloc": (ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(GmConfig), ctypes.POINTER(GmResult)]),
 }
 
 _lib = None
@@ -231,6 +232,18 @@ def glutton_max(puzzle: NativePuzzle, push_budget: int = 0, timeout_ms: int = 0,
     cfg.device = device
     r = GmResult()
     check(load().emp_glutton_max(puzzle.handle, ctypes.byref(cfg), ctypes.byref(r)))
+    return r
+
+
+def glutton_max_noalloc(puzzle: NativePuzzle, push_budget: int = 0, timeout_ms: int = 0,
+                        device: int = -1) -> GmResult:
+    """emp_glutton_max_noalloc: the same search in the library's fixed device array."""
+    cfg = GmConfig()
+    cfg.push_budget = push_budget
+    cfg.timeout_ms = timeout_ms
+    cfg.device = device
+    r = GmResult()
+    check(load().emp_glutton_max_noalloc(puzzle.handle, ctypes.byref(cfg), ctypes.byref(r)))
     return r
 
 

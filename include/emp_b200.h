@@ -197,6 +197,32 @@ typedef struct emp_gm_result {
  * the best candidate, the same backtracking, the same final board. */
 emp_status emp_glutton_max(emp_puzzle puzzle, const emp_gm_config *config, emp_gm_result *result);
 
+/* The same search as emp_glutton_max, with the same results, but it allocates
+ * no device memory. This entry point has no counterpart in the reference.
+ *
+ * It is for callers that must not allocate once they are running. One example
+ * is a service that sizes its device memory at start-up and must not hit an
+ * out-of-memory error halfway through a job. Another is a loop that shares
+ * the GPU with other streams: cudaFree synchronises the whole device and
+ * would stall them.
+ *
+ * Its device memory is one array of 4,232,448 bytes compiled into this
+ * library, one copy per device. That is enough for every puzzle the library
+ * accepts: up to 256 pieces and colour ids up to 31. Larger puzzles are
+ * rejected with EMP_ERR_UNSUPPORTED and a message naming the limit.
+ *
+ * The first call on a device does a one-time set-up: it looks up the array's
+ * device address, which loads the array onto the device. Make that first call
+ * before any stream capture begins.
+ *
+ * Every call shares the array, and the array keeps whatever the previous call
+ * left. Each call rewrites everything the search reads before writing it.
+ * Calls that overlap on the same device, from several host threads, race on
+ * the array: the caller must serialise them.
+ *
+ * kernel_ms is the host's wall time from the launch to the return of the result. */
+emp_status emp_glutton_max_noalloc(emp_puzzle puzzle, const emp_gm_config *config, emp_gm_result *result);
+
 #ifdef __cplusplus
 }
 #endif
