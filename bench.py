@@ -209,7 +209,14 @@ def main():
     ap.add_argument("--full", action="store_true", help="run all slices (the complete count) and print per-seed totals")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
+    ap.add_argument("--seeds", default=None,
+                    help="comma-separated subset of the workload seeds (a smaller case for profiling)")
     args = ap.parse_args()
+    if args.seeds:
+        global SEEDS, WORKLOAD
+        SEEDS = [int(x) for x in args.seeds.split(",")]
+        WORKLOAD = WORKLOAD.replace("16 seeded", f"{len(SEEDS)} seeded").replace(
+            "seeds 0..15", "seeds " + ",".join(map(str, SEEDS)))
     rank = env_int("RANK", 0)
     world = env_int("WORLD_SIZE", 1)
     local_rank = env_int("LOCAL_RANK", 0)

@@ -1,0 +1,199 @@
+// C++ host layer over the C ABI: features, factory, parser, strategy generators.
+#include "emp_host.h"
+
+#include <chrono>
+#include <fstream>
+#include <sstream>
+
+namespace edge_matching_puzzle {
+
+namespace {
+
+[[noreturn]] void throw_abi(const char* call, emp_status status, unsigned line)
+{
+    std::ostringstream s;
+    s << call << " failed (status " << status << "): " << emp_last_error();
+    throw emp_logic_error(s.str(), line, __FILE__);
+}
+
+std::string trim(const std::string& s)
+{
+    size_t b = s.find_first_not_of(" \t\r\n"), e = s.find_last_not_of(" \t\r\n");
+    return b == std::string::npos ? std::string() : s.substr(b, e - b + 1);
+}
+
+}  // namespace
+
+emp_piece_set parse_pieces(const std::string& path)
+{
+    std::ifstream in(path);
+    if (!in) throw emp_logic_error("Unable to open file \"" + path + "\" for reading", __LINE__, __FILE__);
+    std::string line;
+    if (!std::getline(in, line) || trim(line) != "Width,Height")
+        throw emp_logic_error("Bad header line in \"" + path + "\": expected Width,Height", __LINE__, __FILE__);
+    emp_piece_set set;
+    if (!std::getline(in, line) || std::sscanf(line.c_str(), "%u,%u", &set.width, &set.height) != 2)
+        throw emp_logic_error("Bad dimension line in \"" + path + "\"", __LINE__, __FILE__);
+    if (!std::getline(in, line) || trim(line) != "I,N,E,S,O")
+        throw emp_logic_error("Bad header line in \"" + path + "\": expected I,N,E,S,O", __LINE__, __FILE__);
+    const uint64_t n = static_cast<uint64_t>(set.width) * set.height;
+    if (!set.width || !set.height || n > 256)
+        throw emp_logic_error("Unsupported puzzle dimensions in \"" + path + "\"", __LINE__, __FILE__);
+    set.colours.assign(4 * n, 0);
+    std::vector<bool> seen(n, false);
+    uint32_t count = 0;
+    while (std::getline(in, line)) {
+        if (trim(line).empty()) continue;
+        unsigned id, c[4];
+        if (std::sscanf(line.c_str(), "%u,%u,%u,%u,%u", &id, &c[0], &c[1], &c[2], &c[3]) != 5)
+            throw emp_logic_error("Bad piece line \"" + trim(line) + "\" in \"" + path + "\"", __LINE__, __FILE__);
+        if (!id || id > n || seen[id - 1])
+            throw emp_logic_error("Bad piece id " + std::to_string(id) + " in \"" + path + "\"", __LINE__, __FILE__);
+        seen[id - 1] = true;
+        for (unsigned s = 0; s < 4; ++s) {
+            if (c[s] > 255) throw emp_logic_error("Bad colour in \"" + path + "\"", __LINE__, __FILE__);
+            set.colours[4 * (id - 1) + s] = static_cast<uint8_t>(c[s]);
+        }
+        ++count;
+    }
+    if (count != n) {
+        std::ostringstream s;
+        s << "Inconsistency between puzzle dimensions (" << set.width << "*" << set.height << ") and piece number ("
+          << count << ")";
+        throw emp_logic_error(s.str(), __LINE__, __FILE__);
+    }
+    return set;
+}
+
+std::unique_ptr<emp_strategy_generator> create_strategy_generator(const std::string& name, uint32_t width,
+                                                                  uint32_t height)
+{
+    const uint32_t n = width * height;
+    std::vector<uint16_t> order;
+    order.reserve(n);
+    if (name == "basic") {
+        for (uint32_t i = 0; i < n; ++i) order.push_back(static_cast<uint16_t>(i));
+    } else if (name == "spiral") {
+        // walk the frame inwards: right along the top, down, left, up, one ring at a time
+        std::vector<bool> used(n, false);
+        uint32_t x = 0, y = 0;
+        for (uint32_t i = 0; i < n; ++i) {
+            used[y * width + x] = true;
+            order.push_back(static_cast<uint16_t>(y * width + x));
+            if (i + 1 == n) break;
+            if (x >= y) {
+                if (x + 1 < width && !used[y * width + x + 1]) ++x;
+                else if (y + 1 < height && !used[(y + 1) * width + x]) ++y;
+                else --x;
+            } else {
+                if (x && !used[y * width + x - 1]) --x;
+                else if (y && !used[(y - 1) * width + x]) --y;
+                else ++x;
+            }
+        }
+    } else {
+        throw emp_logic_error("Unsupported strategy \"" + name + "\"", __LINE__, __FILE__);
+    }
+    return std::make_unique<emp_strategy_generator>(name, width, height, std::move(order));
+}
+
+std::string situation_string(uint32_t width, uint32_t height, const uint32_t* cells)
+{
+    const uint32_t n = width * height;
+    const size_t digits = std::to_string(n).size();
+    std::string out;
+    out.reserve(n * (digits + 1));
+    for (uint32_t pos = 0; pos < n; ++pos) {
+        const uint32_t c = cells[pos];
+        if (c == 0xFFFFFFFFu) {
+            out.append(digits + 1, '-');
+        } else {
+            const std::string id = std::to_string((c >> 2) + 1);
+            out.append(digits - id.size(), ' ');
+            out += id;
+            out += "NESW"[c & 3u];
+        }
+    }
+    return out;
+}
+
+emp_puzzle_owner::emp_puzzle_owner(const emp_piece_set& pieces, const emp_strategy_generator* strategy)
+{
+    emp_puzzle_desc desc{};
+    desc.width = pieces.width;
+    desc.height = pieces.height;
+    desc.colours = pieces.colours.data();
+    desc.order = strategy ? strategy->order().data() : nullptr;
+    const emp_status st = emp_puzzle_create(&desc, &m_puzzle);
+    if (st != EMP_OK) throw_abi("emp_puzzle_create", st, __LINE__);
+}
+
+emp_puzzle_owner::~emp_puzzle_owner() { emp_puzzle_destroy(m_puzzle); }
+
+feature_CUDA_backtracker::feature_CUDA_backtracker(const emp_piece_set& pieces, const emp_strategy_generator& strategy,
+                                                   const feature_options& options, std::ostream& out)
+    : m_pieces(pieces), m_strategy(strategy), m_options(options), m_out(out)
+{
+}
+
+void feature_CUDA_backtracker::run()
+{
+    const auto start = std::chrono::steady_clock::now();
+    emp_puzzle_owner puzzle(m_pieces, &m_strategy);
+    emp_bt_config cfg{};
+    cfg.device = m_options.device;
+    cfg.split_depth = m_options.split_depth;
+    cfg.stop_at_first = m_options.stop_at_first ? 1u : 0u;
+    cfg.timeout_ms = m_options.timeout_ms;
+    m_out << "Launch kernels" << std::endl;
+    const emp_status st = emp_bt_count(puzzle.get(), &cfg, &m_result);
+    if (st < 0) throw_abi("emp_bt_count", st, __LINE__);
+    // the first solution in visiting order, as the reference's backtracker prints it
+    if (m_result.has_first_solution)
+        m_out << situation_string(m_pieces.width, m_pieces.height, m_result.first_solution) << std::endl;
+    if (st == EMP_INCOMPLETE) m_out << "Search stopped before the end (status " << m_result.status << ")" << std::endl;
+    m_out << "End of algorithm" << std::endl;
+    m_out << "Total situations explored : " << m_result.nodes << std::endl;
+    m_out << "Nb solutions : " << m_result.solutions << std::endl;
+    const std::chrono::duration<double> elapsed = std::chrono::steady_clock::now() - start;
+    m_out << "Total elapsed time: " << elapsed.count() << "s" << std::endl;
+}
+
+feature_CUDA_glutton_max::feature_CUDA_glutton_max(const emp_piece_set& pieces, const feature_options& options,
+                                                   std::ostream& out)
+    : m_pieces(pieces), m_options(options), m_out(out)
+{
+}
+
+void feature_CUDA_glutton_max::run()
+{
+    emp_puzzle_owner puzzle(m_pieces, nullptr);
+    emp_gm_config cfg{};
+    cfg.device = m_options.device;
+    cfg.push_budget = m_options.push_budget;
+    cfg.timeout_ms = m_options.timeout_ms;
+    m_out << "Launch kernels" << std::endl;
+    const emp_status st = emp_glutton_max(puzzle.get(), &cfg, &m_result);
+    if (st < 0) throw_abi("emp_glutton_max", st, __LINE__);
+    if (m_result.status == 2) {
+        m_out << "Empty stack" << std::endl;
+    } else {
+        m_out << "Situation with stack played info:" << std::endl;
+        m_out << situation_string(m_pieces.width, m_pieces.height, m_result.final_board) << std::endl;
+    }
+    m_out << "Max level : " << m_result.max_level << std::endl;
+}
+
+feature_if& factory_feature::create_feature(const std::string& feature_name, const emp_piece_set& pieces,
+                                            std::unique_ptr<emp_strategy_generator>& strategy,
+                                            const feature_options& options, std::ostream& out)
+{
+    if (feature_name == "CUDA_backtracker") {
+        if (!strategy) strategy = create_strategy_generator("basic", pieces.width, pieces.height);
+        return *new feature_CUDA_backtracker(pieces, *strategy, options, out);
+    }
+    if (feature_name == "CUDA_glutton_max") return *new feature_CUDA_glutton_max(pieces, options, out);
+    throw emp_logic_error("Unsupported feature \"" + feature_name + "\"", __LINE__, __FILE__);
+}
+
+}  // namespace edge_matching_puzzle

@@ -1,0 +1,161 @@
+// C++ host layer over the C ABI of include/emp_b200.h.
+//
+// It mirrors the reference's plugin interface for its two GPU searches, with the
+// same class names, constructor arguments and error behaviour, so that a program
+// written against the reference's features reads the same here:
+//
+//   feature_if                  include/feature_if.h:27-33
+//   feature_CUDA_backtracker    include/feature_CUDA_backtracker.h:33-72,
+//                               src/feature_CUDA_backtracker.cpp:31-38
+//   feature_CUDA_glutton_max    include/feature_CUDA_glutton_max.h:31-75
+//   factory_feature             include/factory_feature.h:142-164
+//   emp_pieces_parser::parse    include/emp_pieces_parser.h:53-101
+//   strategy generators         include/emp_basic_strategy_generator.h:44-53 (basic),
+//                               include/emp_spiral_strategy_generator.h:52-100 (spiral)
+//   board strings               include/situation_string_formatter.h:51-70
+//
+// Where the reference throws quicky_exception::quicky_logic_exception, this layer
+// throws emp_logic_error with the same what()/file/line triple; the CLI (main.cpp)
+// catches it and exits with -1 as src/main.cpp:137-146 does.
+#pragma once
+
+#include "emp_b200.h"
+
+#include <cstdint>
+#include <iostream>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <utility>
+#include <vector>
+
+namespace edge_matching_puzzle {
+
+class emp_logic_error : public std::logic_error {
+  public:
+    emp_logic_error(const std::string& what, unsigned line, const char* file)
+        : std::logic_error(what), m_line(line), m_file(file)
+    {
+        const size_t slash = m_file.find_last_of('/');  // keep the file name only
+        if (slash != std::string::npos) m_file.erase(0, slash + 1);
+    }
+    unsigned get_line() const { return m_line; }
+    const std::string& get_file() const { return m_file; }
+
+  private:
+    unsigned m_line;
+    std::string m_file;
+};
+
+// Pieces of a puzzle definition file: colours[4*(id-1)+side], sides N,E,S,W, 0 = frame.
+struct emp_piece_set {
+    uint32_t width = 0;
+    uint32_t height = 0;
+    std::vector<uint8_t> colours;
+    uint32_t size() const { return static_cast<uint32_t>(colours.size() / 4); }
+};
+
+// Reads the reference's CSV puzzle format ("Width,Height" / "w,h" / "I,N,E,S,O" / one
+// line per piece).  Throws emp_logic_error on an unreadable or malformed file.
+emp_piece_set parse_pieces(const std::string& path);
+
+// Visiting order of the positions (the reference's emp_strategy_generator).
+class emp_strategy_generator {
+  public:
+    emp_strategy_generator(std::string name, uint32_t width, uint32_t height, std::vector<uint16_t> order)
+        : m_name(std::move(name)), m_width(width), m_height(height), m_order(std::move(order)) {}
+    const std::string& get_name() const { return m_name; }
+    // (x, y) of the index-th visited position
+    std::pair<unsigned, unsigned> get_position(unsigned index) const
+    {
+        return {m_order.at(index) % m_width, m_order.at(index) / m_width};
+    }
+    const std::vector<uint16_t>& order() const { return m_order; }
+    uint32_t get_width() const { return m_width; }
+    uint32_t get_height() const { return m_height; }
+
+  private:
+    std::string m_name;
+    uint32_t m_width, m_height;
+    std::vector<uint16_t> m_order;
+};
+
+// "basic" (row major) or "spiral"; anything else throws, as emp_strategy_generator_factory does.
+std::unique_ptr<emp_strategy_generator> create_strategy_generator(const std::string& name, uint32_t width,
+                                                                  uint32_t height);
+
+// The reference's board string: per position y*w+x the piece id right-aligned on
+// digits(w*h) characters plus N/E/S/W, or dashes when empty.  cells[pos] holds
+// (id-1)<<2 | orientation, or 0xFFFFFFFF when empty.
+std::string situation_string(uint32_t width, uint32_t height, const uint32_t* cells);
+
+class feature_if {
+  public:
+    virtual void run() = 0;
+    virtual ~feature_if() = default;
+};
+
+// Settings the reference hard-codes; the defaults reproduce its behaviour.
+struct feature_options {
+    bool stop_at_first = false;     // backtracker: stop at the first solution found
+    uint32_t split_depth = 0;       // backtracker: 0 = library default
+    uint64_t push_budget = 0;       // glutton: stop after this many placements (0 = none)
+    uint32_t timeout_ms = 0;        // 0 = library default
+    int device = -1;                // CUDA device, -1 = current
+};
+
+// Owns an emp_puzzle built from a piece set and an optional visiting order.
+class emp_puzzle_owner {
+  public:
+    emp_puzzle_owner(const emp_piece_set& pieces, const emp_strategy_generator* strategy);
+    ~emp_puzzle_owner();
+    emp_puzzle_owner(const emp_puzzle_owner&) = delete;
+    emp_puzzle_owner& operator=(const emp_puzzle_owner&) = delete;
+    emp_puzzle get() const { return m_puzzle; }
+
+  private:
+    emp_puzzle m_puzzle = nullptr;
+};
+
+// Exhaustive count of all solutions in the strategy's position order (emp_strategy's
+// node and solution accounting), printing the first solution's board and the totals.
+class feature_CUDA_backtracker : public feature_if {
+  public:
+    feature_CUDA_backtracker(const emp_piece_set& pieces, const emp_strategy_generator& strategy,
+                             const feature_options& options = {}, std::ostream& out = std::cout);
+    void run() override;
+    const emp_bt_result& get_result() const { return m_result; }
+
+  private:
+    const emp_piece_set& m_pieces;
+    const emp_strategy_generator& m_strategy;
+    feature_options m_options;
+    std::ostream& m_out;
+    emp_bt_result m_result{};
+};
+
+// Greedy max-placement search, printing the final board as launch_CUDA_glutton_max does.
+class feature_CUDA_glutton_max : public feature_if {
+  public:
+    feature_CUDA_glutton_max(const emp_piece_set& pieces, const feature_options& options = {},
+                             std::ostream& out = std::cout);
+    void run() override;
+    const emp_gm_result& get_result() const { return m_result; }
+
+  private:
+    const emp_piece_set& m_pieces;
+    feature_options m_options;
+    std::ostream& m_out;
+    emp_gm_result m_result{};
+};
+
+class factory_feature {
+  public:
+    // Creates the feature by name ("CUDA_backtracker", "CUDA_glutton_max").  The
+    // caller owns the returned object.  Other names throw "Unsupported feature".
+    static feature_if& create_feature(const std::string& feature_name, const emp_piece_set& pieces,
+                                      std::unique_ptr<emp_strategy_generator>& strategy,
+                                      const feature_options& options = {}, std::ostream& out = std::cout);
+};
+
+}  // namespace edge_matching_puzzle

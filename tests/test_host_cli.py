@@ -1,0 +1,102 @@
+"""The C++ host layer (edge_matching_puzzle_b200/csrc/host) through its command line,
+checked the way the reference's own tests check its binary: the arguments of
+tests/*/test.info and the stdout lines they expect.
+
+CPU tests cover argument handling and error behaviour (ERROR line, exit code -1, as
+src/main.cpp:137-146); GPU tests run the two CUDA features on the reference examples."""
+from __future__ import annotations
+
+import os
+import subprocess
+
+import pytest
+
+from edge_matching_puzzle_b200 import build as native_build
+
+CLI = native_build.CLI
+
+
+@pytest.fixture(scope="module")
+def cli():
+    if not os.path.exists(CLI):
+        native_build.build()
+    assert os.path.exists(CLI), "the host command line was not built"
+    return CLI
+
+
+@pytest.fixture()
+def example(tmp_path, reference_vectors):
+    def write(name):
+        path = tmp_path / f"{name}.txt"
+        path.write_text(reference_vectors["puzzles"][name])
+        return str(path)
+    return write
+
+
+def run(cli, *args, timeout=300):
+    r = subprocess.run([cli, *args], capture_output=True, text=True, timeout=timeout)
+    return r.returncode, r.stdout.splitlines()
+
+
+def test_unsupported_feature(cli, example):
+    rc, out = run(cli, example("3_3"), "ressources", "no_such_feature", "--enable_gui=false")
+    assert rc == 255
+    assert out[0] == "9 pieces loaded"
+    assert out[-1].startswith('ERROR : Unsupported feature "no_such_feature" at ')
+
+
+def test_missing_definition_file(cli, tmp_path):
+    rc, out = run(cli, str(tmp_path / "missing.txt"), "ressources", "CUDA_backtracker")
+    assert rc == 255 and out[-1].startswith("ERROR : Unable to open file")
+
+
+def test_piece_count_mismatch(cli, tmp_path, reference_vectors):
+    lines = reference_vectors["puzzles"]["3_3"].strip().splitlines()
+    path = tmp_path / "short.txt"
+    path.write_text("\n".join(lines[:-1]) + "\n")
+    rc, out = run(cli, str(path), "ressources", "CUDA_glutton_max")
+    assert rc == 255 and "Inconsistency between puzzle dimensions (3*3) and piece number (8)" in out[-1]
+
+
+@pytest.mark.parametrize("args,msg", [
+    (["--strategy=zigzag"], 'Unsupported strategy "zigzag"'),
+    (["--colour=3"], 'Unknown parameter "colour"'),
+    (["--stop_at_first=maybe"], 'Bad boolean value "maybe"'),
+])
+def test_bad_options(cli, example, args, msg):
+    rc, out = run(cli, example("3_3"), "ressources", "CUDA_backtracker", *args)
+    assert rc == 255 and msg in out[-1]
+
+
+def test_usage(cli):
+    rc, out = run(cli)
+    assert rc == 255 and "usage" in out[-1]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["3_3", "4_4", "5_5"])
+def test_glutton_max_reference_lines(cli, example, reference_vectors, name):
+    """tests/CUDA_glutton_max_<name>/test.info: Launch kernels, the header line, the board."""
+    rc, out = run(cli, example(name), "ressources", "CUDA_glutton_max", "--enable_gui=false")
+    assert rc == 0, out
+    expected = reference_vectors["glutton_max"][name]
+    pos = 0
+    for line in out:
+        if pos < len(expected) and line == expected[pos]:
+            pos += 1
+    assert pos == len(expected), (expected, out)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["3_3", "4_4", "5_5"])
+def test_backtracker_first_solution_and_totals(cli, example, reference_vectors, name):
+    """tests_CUDA/backtracker_<name>: the first solution board (row-major order); with the
+    spiral order, the totals of tests/new_strategy_<name>."""
+    rc, out = run(cli, example(name), "ressources", "CUDA_backtracker", "--enable_gui=false")
+    assert rc == 0, out
+    assert reference_vectors["backtracker_first_solution"][name] in out
+    rc, out = run(cli, example(name), "ressources", "CUDA_backtracker", "--strategy=spiral")
+    assert rc == 0, out
+    expected = [l for l in reference_vectors["new_strategy"][name]["expected_stdout"]
+                if l.startswith(("Total situations explored", "Nb solutions"))]
+    assert all(l in out for l in expected), (expected, out)
