@@ -174,6 +174,146 @@ def cpu_sample(threads: int, first: int, stride: int):
     return nodes, seconds, kinds, subtrees
 
 
+BATCH_COUNT = 4096
+BATCH_STEP_MS = 2000
+BATCH_WORKLOAD = (f"batched exhaustive search of {BATCH_COUNT} square puzzles, sides 4..9, 3..5 border / 4..10 "
+                  f"interior colours (splitmix64 stream seed 2); one step = one CUDA graph launch over all "
+                  f"instances with a {BATCH_STEP_MS} ms deadline, launch parameters from the autotuner; "
+                  f"instances that finish are exact, the others flagged incomplete")
+
+
+def _batch_cpu_sample(batch, threads, stride=16, node_limit=20_000_000):
+    """Oracle (CPU restatement of emp_strategy) on instances 0, stride, 2*stride, ... of the
+    batch, each stopped after node_limit placements, one instance per host thread."""
+    import concurrent.futures as cf
+    from oracle.oracle import OraclePuzzle
+    sample = batch[::stride]
+
+    def one(pz):
+        r, _ = OraclePuzzle(pz.width, pz.height, pz.colors).run(node_limit=node_limit)
+        return r.nodes
+    t0 = time.perf_counter()
+    with cf.ThreadPoolExecutor(max_workers=threads) as ex:
+        nodes = sum(ex.map(one, sample))
+    return nodes, time.perf_counter() - t0, len(sample)
+
+
+def run_batch(args, rank, world, local_rank):
+    """The batched mixed-size workload: aggregate placements/s of one graph launch per step."""
+    import torch
+    from edge_matching_puzzle_b200 import native
+    from edge_matching_puzzle_b200.puzzle import mixed_batch
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local_rank))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    batch = mixed_batch(BATCH_COUNT)
+    mine = batch[rank::world]  # instances shard across ranks: no data-path collective
+    handles = [native.NativePuzzle(p.width, p.height, p.colors) for p in mine]
+    tune = native.bt_autotune(handles, trial_ms=400, use_graph=1, table_placement=1, device=local_rank)
+    cfg = native.config_dict(tune.best)
+    cfg.pop("reserved")
+    cfg.update(timeout_ms=BATCH_STEP_MS, use_graph=1, device=local_rank)
+    plan = native.BtPlan(handles, **cfg)
+    flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.int32, device="cuda")
+    start_ev = torch.cuda.Event(enable_timing=True)
+    end_ev = torch.cuda.Event(enable_timing=True)
+    sampler = ClockSampler(torch.cuda.current_device())
+    ms = 0.0
+    nodes = 0
+    rounds = 0
+    res = None
+    for i in range(args.warmup + args.steps):
+        if i == args.warmup:
+            sampler.__enter__()
+        flush.add_(1)
+        barrier()
+        start_ev.record()
+        plan.run(torch.cuda.current_stream().cuda_stream)
+        end_ev.record()
+        barrier()
+        res = plan.results()
+        if i >= args.warmup:
+            ms += start_ev.elapsed_time(end_ev)
+            nodes += sum(r.nodes - r.expansion_nodes for r in res)
+            rounds += res[0].rounds
+    sampler.__exit__()
+    clocks = sampler.summary()
+    complete = sum(1 for r in res if r.status == native.EMP_OK)
+    if args.counts_out and rank == 0:
+        with open(args.counts_out, "w") as f:
+            for j, (pz, r) in enumerate(zip(mine, res)):
+                f.write(json.dumps({"instance": j, "side": pz.width, "nodes": r.nodes, "solutions": r.solutions,
+                                    "complete": r.status == native.EMP_OK, "split_depth": r.split_depth}) + "\n")
+    # end to end: the public one-shot call from host puzzles (tables built, uploaded and
+    # expanded inside the timed region)
+    e_nodes = 0
+    e_sec = 0.0
+    h2d = d2h = 0
+    for i in range(1 + (args.steps if not args.no_e2e else 0)):
+        barrier()
+        t0 = time.perf_counter()
+        hp = [native.NativePuzzle(p.width, p.height, p.colors) for p in mine]
+        er = native.bt_count_batch(hp, **cfg)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        if i >= 1:
+            e_nodes += sum(r.nodes for r in er)
+            e_sec += dt
+            h2d = sum(p.table_bytes() for p in hp) + 12 * len(hp)
+            d2h = len(hp) * (16 + 8 + 4 + 528)
+        for p in hp:
+            p.close()
+    if dist is not None:
+        t = torch.tensor([ms, float(nodes), e_sec, float(e_nodes), float(complete)], dtype=torch.float64, device="cuda")
+        mx = t.clone()
+        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        ms, nodes, e_sec, e_nodes, complete = mx[0].item(), t[1].item(), mx[2].item(), t[3].item(), int(t[4].item())
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        threads = os.cpu_count() or 1
+        cn, csec, cnt = _batch_cpu_sample(batch, threads)
+        cpu = {"value": cn / csec, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": f"{cnt} instances (every 16th), each stopped after 2e7 placements, CPU oracle "
+                         f"(restatement of emp_strategy), one instance per host thread"}
+    if rank == 0:
+        peaks, peak_kind = measured_peaks()
+        out = {
+            "metric": METRIC, "value": nodes / (ms / 1000.0), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+            "config": {"workload": BATCH_WORKLOAD, "instances": BATCH_COUNT,
+                       "parallelism": f"{world} GPU(s), instances sharded",
+                       "l2": "flushed between steps (252 MB write)", "tuned": cfg,
+                       "autotune": {"trials": tune.trials, "best_rate": tune.best_rate,
+                                    "default_rate": tune.default_rate}},
+            "gpu_launches": args.steps * (3 + 3 * max(rounds // max(args.steps, 1), 1)),
+            "instances_complete": complete,
+            "roofline": {"bound": "hbm", "achieved": None, "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": None,
+                         "traffic": None, "peak_source": peak_kind,
+                         "note": "the DFS keeps its state on chip and reads tables through L1/L2 (66 MB of tables "
+                                 "fit L2); the 8x8 workload carries the on-chip roofline"},
+            "clocks": clocks,
+            "e2e": {"value": e_nodes / e_sec if e_sec else None, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "cpu_baseline": cpu,
+            "dfs": {"rounds_per_step": rounds / args.steps},
+        }
+        print(json.dumps(out), flush=True)
+    plan.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -209,6 +349,9 @@ def main():
     ap.add_argument("--full", action="store_true", help="run all slices (the complete count) and print per-seed totals")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
+    ap.add_argument("--workload", default="exhaustive", choices=["exhaustive", "batch"],
+                    help="exhaustive: the 16 seeded 8x8 puzzles (default); batch: 4096 mixed instances")
+    ap.add_argument("--counts-out", default=None, help="batch: write per-instance counts (JSON lines) here")
     ap.add_argument("--seeds", default=None,
                     help="comma-separated subset of the workload seeds (a smaller case for profiling)")
     args = ap.parse_args()
@@ -222,6 +365,9 @@ def main():
     local_rank = env_int("LOCAL_RANK", 0)
     if args.impl == "reference":
         run_reference(args, rank, world)
+        return
+    if args.workload == "batch":
+        run_batch(args, rank, world, local_rank)
         return
 
     import torch

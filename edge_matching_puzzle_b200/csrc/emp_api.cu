@@ -102,6 +102,13 @@ struct emp_bt_plan_t {
     DeviceBuffer rec_init, rec_a, rec_b;      // initial records (selection), round queues
     DeviceBuffer counters;                    // [0] cursor, [1] output tail
     DeviceBuffer totals, first_item, records, flags, item_nodes, item_sols, spill, prefix_out;
+    DeviceBuffer ctl, incomplete, puzzle_depth_dev;
+    std::vector<uint32_t> puzzle_depth;       // per puzzle split depth
+    bool adaptive = false;                    // per puzzle split depths (split_subtrees)
+    cudaStream_t capture_stream = nullptr;    // graph runs: stream the graph is captured on
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
+    bool graph_ran = false;
     uint64_t n_all = 0, n_init = 0;
     bool sampled = false;
     std::vector<unsigned long long> exp_nodes, exp_sols;
@@ -111,8 +118,18 @@ struct emp_bt_plan_t {
     double busy_ms = 0;
     uint64_t records_in = 0, records_out = 0;
 
+    void drop_graph()
+    {
+        if (graph_exec) cudaGraphExecDestroy(graph_exec);
+        if (graph) cudaGraphDestroy(graph);
+        graph_exec = nullptr;
+        graph = nullptr;
+    }
+
     ~emp_bt_plan_t()
     {
+        drop_graph();
+        if (capture_stream) cudaStreamDestroy(capture_stream);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
         if (evr0) cudaEventDestroy(evr0);
@@ -146,6 +163,8 @@ struct emp_bt_plan_t {
         P.abort_flag = flags.as<int>();
         P.status = flags.as<int>() + 1;
         P.stop_at_first = cfg.stop_at_first ? 1 : 0;
+        P.ctl = ctl.as<emp::BtRunCtl>();
+        P.incomplete = incomplete.as<uint32_t>();
         return P;
     }
 };
@@ -170,20 +189,48 @@ emp_status expand(emp_bt_plan_t& pl)
     CUDA_TRY(cudaMemsetAsync(lv.p, 0, lv.bytes, st));
     CUDA_TRY(parent_puzzle.alloc(sizeof(uint32_t) * P));
     {
+        // subtrees are queued puzzle by puzzle, smaller puzzles first: under a
+        // deadline the cheap instances of a mixed batch finish before the threads
+        // are taken by large ones (within a puzzle, subtrees stay in search order)
         std::vector<uint32_t> ids(P);
         for (uint32_t i = 0; i < P; ++i) ids[i] = i;
+        std::stable_sort(ids.begin(), ids.end(), [&](uint32_t a, uint32_t b) {
+            return pl.puzzles[a]->model.n < pl.puzzles[b]->model.n;
+        });
         CUDA_TRY(cudaMemcpyAsync(parent_puzzle.p, ids.data(), sizeof(uint32_t) * P, cudaMemcpyHostToDevice, st));
+        CUDA_TRY(cudaStreamSynchronize(st));
     }
     CUDA_TRY(parents.alloc(2));
     CUDA_TRY(grand.alloc(sizeof(uint64_t)));
     uint64_t np = P;
     unsigned long long* lnodes = lv.as<unsigned long long>();
-    for (uint32_t level = 0; level < pl.depth; ++level) {
+    // per puzzle split depths: a puzzle stops expanding (is frozen) once it has
+    // split_subtrees prefixes, reaches its depth limit or runs out of prefixes
+    DeviceBuffer frozen_dev;
+    std::vector<uint8_t> frozen(P, 0);
+    std::vector<uint32_t> cap(P);
+    std::vector<unsigned long long> seen(P, 0), now(P, 0);
+    uint32_t levels = pl.depth;
+    pl.puzzle_depth.assign(P, pl.depth);
+    if (pl.adaptive) {
+        CUDA_TRY(frozen_dev.alloc(P));
+        CUDA_TRY(cudaMemsetAsync(frozen_dev.p, 0, P, st));
+        levels = 0;
+        for (uint32_t i = 0; i < P; ++i) {
+            const uint32_t lim = pl.cfg.split_depth ? std::min<uint32_t>(pl.cfg.split_depth, 64u) : 64u;
+            cap[i] = std::max<uint32_t>(1u, std::min<uint32_t>(lim, pl.puzzles[i]->model.n - 1));
+            levels = std::max(levels, cap[i]);
+        }
+    }
+    uint32_t level = 0;
+    for (; level < levels; ++level) {
         CUDA_TRY(counts.alloc(sizeof(uint32_t) * std::max<uint64_t>(np, 1)));
         CUDA_TRY(offsets.alloc(sizeof(uint64_t) * std::max<uint64_t>(np, 1)));
         CUDA_TRY(bsums.alloc(sizeof(uint64_t) * emp::scan_block_sum_words(np)));
-        CUDA_TRY(emp::launch_expand(L, parents.as<uint16_t>(), parent_puzzle.as<uint32_t>(), np, level,
-                                    counts.as<uint32_t>(), nullptr, nullptr, nullptr, lnodes, lnodes + P, 0, st));
+        const uint8_t* fz = pl.adaptive ? frozen_dev.as<uint8_t>() : nullptr;
+        CUDA_TRY(emp::launch_expand_frozen(L, parents.as<uint16_t>(), parent_puzzle.as<uint32_t>(), np, level,
+                                           counts.as<uint32_t>(), nullptr, nullptr, nullptr, lnodes, lnodes + P, 0,
+                                           fz, st));
         CUDA_TRY(emp::launch_scan(counts.as<uint32_t>(), np, offsets.as<uint64_t>(), bsums.as<uint64_t>(),
                                   grand.as<uint64_t>(), st));
         uint64_t total = 0;
@@ -191,20 +238,50 @@ emp_status expand(emp_bt_plan_t& pl)
         CUDA_TRY(cudaStreamSynchronize(st));
         CUDA_TRY(children.alloc(sizeof(uint16_t) * std::max<uint64_t>(total, 1) * (level + 1)));
         CUDA_TRY(child_puzzle.alloc(sizeof(uint32_t) * std::max<uint64_t>(total, 1)));
-        CUDA_TRY(emp::launch_expand(L, parents.as<uint16_t>(), parent_puzzle.as<uint32_t>(), np, level,
-                                    counts.as<uint32_t>(), offsets.as<uint64_t>(), children.as<uint16_t>(),
-                                    child_puzzle.as<uint32_t>(), lnodes, lnodes + P, 1, st));
+        CUDA_TRY(emp::launch_expand_frozen(L, parents.as<uint16_t>(), parent_puzzle.as<uint32_t>(), np, level,
+                                           counts.as<uint32_t>(), offsets.as<uint64_t>(), children.as<uint16_t>(),
+                                           child_puzzle.as<uint32_t>(), lnodes, lnodes + P, 1, fz, st));
         std::swap(parents, children);
         std::swap(parent_puzzle, child_puzzle);
         np = total;
-        if (!np) break;
+        if (pl.adaptive) {
+            // placements of this level per puzzle = its prefixes after this level
+            CUDA_TRY(cudaMemcpyAsync(now.data(), lnodes, sizeof(unsigned long long) * P, cudaMemcpyDeviceToHost, st));
+            CUDA_TRY(cudaStreamSynchronize(st));
+            bool all = true;
+            for (uint32_t i = 0; i < P; ++i) {
+                if (frozen[i]) continue;
+                const unsigned long long prefixes = now[i] - seen[i];
+                seen[i] = now[i];
+                pl.puzzle_depth[i] = level + 1;
+                if (prefixes >= pl.cfg.split_subtrees || level + 1 >= cap[i] || !prefixes) frozen[i] = 1;
+                all = all && frozen[i];
+            }
+            CUDA_TRY(cudaMemcpyAsync(frozen_dev.p, frozen.data(), P, cudaMemcpyHostToDevice, st));
+            CUDA_TRY(cudaStreamSynchronize(st));
+            if (all) {
+                ++level;
+                break;
+            }
+        }
+        if (!np) {
+            ++level;
+            break;
+        }
     }
+    if (pl.adaptive) pl.depth = level;
     pl.exp_nodes.assign(P, 0);
     pl.exp_sols.assign(P, 0);
     CUDA_TRY(cudaMemcpyAsync(pl.exp_nodes.data(), lnodes, sizeof(unsigned long long) * P, cudaMemcpyDeviceToHost, st));
     CUDA_TRY(cudaMemcpyAsync(pl.exp_sols.data(), lnodes + P, sizeof(unsigned long long) * P, cudaMemcpyDeviceToHost, st));
     CUDA_TRY(cudaStreamSynchronize(st));
     pl.n_all = np;
+    if (pl.adaptive) {
+        CUDA_TRY(pl.puzzle_depth_dev.alloc(sizeof(uint32_t) * P));
+        CUDA_TRY(cudaMemcpyAsync(pl.puzzle_depth_dev.p, pl.puzzle_depth.data(), sizeof(uint32_t) * P,
+                                 cudaMemcpyHostToDevice, st));
+        CUDA_TRY(cudaStreamSynchronize(st));
+    }
     pl.prefixes = std::move(parents);
     pl.prefix_puzzle = std::move(parent_puzzle);
     return EMP_OK;
@@ -215,7 +292,8 @@ emp_status build_initial(emp_bt_plan_t& pl, uint64_t first, uint64_t stride, uin
 {
     CUDA_TRY(pl.rec_init.alloc(sizeof(uint32_t) * pl.rec_words * std::max<uint64_t>(count, 1)));
     CUDA_TRY(emp::launch_make_records(pl.prefixes.as<uint16_t>(), pl.prefix_puzzle.as<uint32_t>(), pl.depth, first,
-                                      stride, count, pl.rec_words, pl.rec_init.as<uint32_t>(), nullptr));
+                                      stride, count, pl.rec_words, pl.rec_init.as<uint32_t>(), nullptr,
+                                      pl.adaptive ? pl.puzzle_depth_dev.as<uint32_t>() : nullptr));
     if (pl.cfg.keep_subtree_counts) {
         CUDA_TRY(pl.item_nodes.alloc(sizeof(unsigned long long) * std::max<uint64_t>(count, 1)));
         CUDA_TRY(pl.item_sols.alloc(sizeof(unsigned long long) * std::max<uint64_t>(count, 1)));
@@ -248,9 +326,14 @@ extern "C" emp_status emp_bt_plan_create(const emp_puzzle* puzzles, uint32_t cou
         pl->max_avail = std::max(pl->max_avail, t.avail_words);
         pl->max_kw = std::max(pl->max_kw, t.max_kw);
     }
+    pl->adaptive = pl->cfg.split_subtrees != 0;
     pl->depth = pl->cfg.split_depth ? pl->cfg.split_depth : auto_depth(min_n);
-    if (pl->depth >= min_n || pl->depth > 64)
+    if (pl->adaptive) {
+        if (pl->cfg.split_depth > 64)
+            return fail(EMP_ERR_INVALID, "emp_bt_plan_create: split depth limit must be at most 64");
+    } else if (pl->depth >= min_n || pl->depth > 64) {
         return fail(EMP_ERR_INVALID, "emp_bt_plan_create: split depth must be below the piece count and at most 64");
+    }
     pl->rec_words = emp::record_words(pl->max_levels, pl->max_kw);
     EMP_TRY(emp::select_device(pl->cfg.device, &pl->device));
     // tables
@@ -269,11 +352,14 @@ extern "C" emp_status emp_bt_plan_create(const emp_puzzle* puzzles, uint32_t cou
     CUDA_TRY(pl->first_item.alloc(sizeof(unsigned long long) * count));
     CUDA_TRY(pl->records.alloc(sizeof(emp::FirstRecord) * count));
     CUDA_TRY(pl->flags.alloc(2 * sizeof(int)));
+    CUDA_TRY(pl->ctl.alloc(sizeof(emp::BtRunCtl)));
+    CUDA_TRY(pl->incomplete.alloc(sizeof(uint32_t) * count));
     CUDA_TRY(pl->prefix_out.alloc(sizeof(uint16_t) * 256));
     CUDA_TRY(cudaEventCreate(&pl->ev0));
     CUDA_TRY(cudaEventCreate(&pl->ev1));
     CUDA_TRY(cudaEventCreate(&pl->evr0));
     CUDA_TRY(cudaEventCreate(&pl->evr1));
+    if (pl->cfg.use_graph) CUDA_TRY(cudaStreamCreateWithFlags(&pl->capture_stream, cudaStreamNonBlocking));
     EMP_TRY(expand(*pl));
     // hot tables in shared memory when the plan holds one puzzle
     const uint32_t hot = (pl->puzzles[0]->tables.blob[26] + 3u) & ~3u;
@@ -336,10 +422,79 @@ extern "C" emp_status emp_bt_plan_select(emp_bt_plan plan, uint64_t first, uint6
     if (count && first + (count - 1) * stride >= plan->n_all)
         return fail(EMP_ERR_INVALID, "emp_bt_plan_select: selection past the last subtree");
     CUDA_TRY(cudaSetDevice(plan->device));
+    plan->drop_graph();  // the graph holds the previous selection's records
     EMP_TRY(build_initial(*plan, first, stride, count));
     plan->sampled = true;
     return EMP_OK;
 }
+
+namespace {
+
+constexpr uint32_t kMaxRounds = 100000;
+
+// The whole run as one graph:
+//   reset -> zero the queue counters -> DFS round 1 (initial records) -> advance
+//   -> while (records were handed back) { copy them to the input queue -> DFS -> advance }
+// The advance kernel sets the loop's condition on the device, so the host
+// launches the graph once and never waits between rounds.
+emp_status build_graph(emp_bt_plan_t& pl)
+{
+    cudaStream_t cs = pl.capture_stream;
+    cudaGraph_t g = nullptr;
+    CUDA_TRY(cudaGraphCreate(&g, 0));
+    pl.graph = g;
+    cudaGraphConditionalHandle loop;
+    CUDA_TRY(cudaGraphConditionalHandleCreate(&loop, g, 0, 0));
+    emp::BtLaunch P = pl.launch();
+    P.in_rec = pl.rec_init.as<uint32_t>();
+    P.n_in = pl.n_init;
+    P.out_rec = pl.rec_b.as<uint32_t>();
+    CUDA_TRY(cudaStreamBeginCaptureToGraph(cs, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    cudaError_t e = emp::launch_bt_reset(P, static_cast<uint32_t>(pl.puzzles.size()), cs);
+    if (e == cudaSuccess) e = cudaMemsetAsync(pl.counters.p, 0, pl.counters.bytes, cs);
+    if (e == cudaSuccess && pl.item_nodes.p) e = cudaMemsetAsync(pl.item_nodes.p, 0, pl.item_nodes.bytes, cs);
+    if (e == cudaSuccess && pl.item_sols.p) e = cudaMemsetAsync(pl.item_sols.p, 0, pl.item_sols.bytes, cs);
+    if (e == cudaSuccess) e = emp::launch_dfs(P, pl.blocks, pl.threads, cs);
+    if (e == cudaSuccess) e = emp::launch_round_advance(P, loop, kMaxRounds, cs);
+    cudaError_t e2 = cudaStreamEndCapture(cs, &g);
+    CUDA_TRY(e);
+    CUDA_TRY(e2);
+    // the loop hangs below the captured chain's last node
+    size_t n = 0;
+    CUDA_TRY(cudaGraphGetNodes(g, nullptr, &n));
+    std::vector<cudaGraphNode_t> nodes(n);
+    CUDA_TRY(cudaGraphGetNodes(g, nodes.data(), &n));
+    cudaGraphNode_t sink = nullptr;
+    for (cudaGraphNode_t nd : nodes) {
+        size_t deps = 0;
+        CUDA_TRY(cudaGraphNodeGetDependentNodes(nd, nullptr, &deps));
+        if (!deps) sink = nd;
+    }
+    if (!sink) return fail(EMP_ERR_CUDA, "graph build: no last node");
+    cudaGraphNodeParams cp{};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = loop;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t cnode;
+    CUDA_TRY(cudaGraphAddNode(&cnode, g, &sink, 1, &cp));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    emp::BtLaunch Q = P;
+    Q.in_rec = pl.rec_a.as<uint32_t>();
+    Q.n_in = 0;
+    Q.n_in_from_ctl = 1;
+    CUDA_TRY(cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    e = emp::launch_round_copy(Q, pl.rec_a.as<uint32_t>(), pl.rec_b.as<uint32_t>(), cs);
+    if (e == cudaSuccess) e = emp::launch_dfs(Q, pl.blocks, pl.threads, cs);
+    if (e == cudaSuccess) e = emp::launch_round_advance(Q, loop, kMaxRounds, cs);
+    e2 = cudaStreamEndCapture(cs, &body);
+    CUDA_TRY(e);
+    CUDA_TRY(e2);
+    CUDA_TRY(cudaGraphInstantiate(&pl.graph_exec, g, 0));
+    return EMP_OK;
+}
+
+}  // namespace
 
 extern "C" emp_status emp_bt_plan_run(emp_bt_plan plan, void* stream)
 {
@@ -347,6 +502,22 @@ extern "C" emp_status emp_bt_plan_run(emp_bt_plan plan, void* stream)
     if (!plan) return fail(EMP_ERR_INVALID, "emp_bt_plan_run: null plan");
     CUDA_TRY(cudaSetDevice(plan->device));
     cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (plan->cfg.use_graph) {
+        if (!plan->graph_exec) {
+            const emp_status s = build_graph(*plan);
+            if (s != EMP_OK) {
+                plan->drop_graph();
+                return s;
+            }
+        }
+        CUDA_TRY(cudaEventRecord(plan->ev0, st));
+        CUDA_TRY(cudaGraphLaunch(plan->graph_exec, st));
+        CUDA_TRY(cudaEventRecord(plan->ev1, st));
+        plan->graph_ran = true;
+        plan->ran = true;
+        return EMP_OK;
+    }
+    plan->graph_ran = false;
     emp::BtLaunch P = plan->launch();
     CUDA_TRY(emp::launch_bt_reset(P, static_cast<uint32_t>(plan->puzzles.size()), st));
     if (plan->item_nodes.p) {
@@ -384,7 +555,7 @@ extern "C" emp_status emp_bt_plan_run(emp_bt_plan plan, void* stream)
         plan->records_out += n_in;
         in = out->as<uint32_t>();
         std::swap(out, spare);
-        if (plan->rounds > 100000) return fail(EMP_ERR_CUDA, "emp_bt_plan_run: too many rounds");
+        if (plan->rounds > kMaxRounds) return fail(EMP_ERR_CUDA, "emp_bt_plan_run: too many rounds");
     }
     CUDA_TRY(cudaEventRecord(plan->ev1, st));
     plan->ran = true;
@@ -407,17 +578,28 @@ extern "C" emp_status emp_bt_plan_results(emp_bt_plan plan, emp_bt_result* resul
     CUDA_TRY(cudaMemcpy(tot.data(), plan->totals.p, sizeof(unsigned long long) * 2 * P, cudaMemcpyDeviceToHost));
     CUDA_TRY(cudaMemcpy(rec.data(), plan->records.p, sizeof(emp::FirstRecord) * P, cudaMemcpyDeviceToHost));
     CUDA_TRY(cudaMemcpy(flags, plan->flags.p, sizeof(flags), cudaMemcpyDeviceToHost));
-    const bool aborted = (flags[1] & (emp::EMP_DEV_ABORTED | emp::EMP_DEV_TIMEOUT)) != 0;
+    std::vector<uint32_t> incomplete(P);
+    CUDA_TRY(cudaMemcpy(incomplete.data(), plan->incomplete.p, sizeof(uint32_t) * P, cudaMemcpyDeviceToHost));
+    (void)flags;
+    if (plan->graph_ran) {
+        emp::BtRunCtl c{};
+        CUDA_TRY(cudaMemcpy(&c, plan->ctl.p, sizeof(c), cudaMemcpyDeviceToHost));
+        if (c.n_in) return fail(EMP_ERR_CUDA, "emp_bt_plan_results: the graph run stopped after too many rounds");
+        plan->rounds = static_cast<uint32_t>(c.rounds);
+        plan->records_in = c.records_in;
+        plan->records_out = c.records_out;
+        plan->busy_ms = ms;
+    }
     for (uint32_t i = 0; i < P; ++i) {
         emp_bt_result& r = results[i];
         std::memset(&r, 0, sizeof(r));
         const emp_puzzle pz = plan->puzzles[i];
         r.subtrees = plan->n_init;
-        r.split_depth = plan->depth;
+        r.split_depth = plan->puzzle_depth.empty() ? plan->depth : plan->puzzle_depth[i];
         r.expansion_nodes = plan->exp_nodes[i];
         r.nodes = tot[2 * i] + (plan->sampled ? 0 : plan->exp_nodes[i]);
         r.solutions = tot[2 * i + 1] + (plan->sampled ? 0 : plan->exp_sols[i]);
-        r.status = aborted ? EMP_INCOMPLETE : EMP_OK;
+        r.status = incomplete[i] ? EMP_INCOMPLETE : EMP_OK;
         r.kernel_ms = ms;
         r.rounds = plan->rounds;
         r.dfs_busy_ms = plan->busy_ms;

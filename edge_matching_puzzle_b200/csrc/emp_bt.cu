@@ -51,11 +51,25 @@ __global__ void expand_kernel(BtLaunch P, const uint16_t* __restrict__ parents,
                               uint32_t level, uint32_t* __restrict__ counts,
                               const uint64_t* __restrict__ offsets, uint16_t* __restrict__ children,
                               uint32_t* __restrict__ child_puzzle, unsigned long long* __restrict__ level_nodes,
-                              unsigned long long* __restrict__ level_sols, int mode)
+                              unsigned long long* __restrict__ level_sols, int mode,
+                              const uint8_t* __restrict__ frozen)
 {
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n_parents;
          i += (uint64_t)gridDim.x * blockDim.x) {
         const uint32_t pz = parent_puzzle ? parent_puzzle[i] : 0u;
+        if (frozen && frozen[pz]) {
+            // this puzzle has enough subtrees: carry the prefix over, padded
+            if (mode) {
+                const uint16_t* pre = parents + i * level;
+                uint16_t* c = children + offsets[i] * (level + 1);
+                for (uint32_t l = 0; l < level; ++l) c[l] = pre[l];
+                c[level] = 0xFFFFu;
+                if (child_puzzle) child_puzzle[offsets[i]] = pz;
+            } else {
+                counts[i] = 1;
+            }
+            continue;
+        }
         const uint32_t* tb = P.tables + P.puzzle_offset[pz];
         const uint32_t n = ldg(tb + H_N), ncol = ldg(tb + H_NCOL), desc_off = ldg(tb + H_DESC);
         uint64_t av[kMaxAvailWords];
@@ -587,7 +601,9 @@ __global__ void __launch_bounds__(T) dfs_kernel(BtLaunch P)
     bool drained = false;      // warp-uniform: the input queue of this round is empty
     uint32_t iteration = 0;    // warp-uniform loop counter
     uint32_t since_check = 0;  // steps since the last look at the global flags
-    const uint64_t deadline = P.timeout_ns ? global_ns() + P.timeout_ns : 0;
+    // the run's deadline (set by reset_kernel) and this round's record count
+    const uint64_t deadline = *(volatile unsigned long long*)&P.ctl->deadline;
+    const uint64_t n_in = P.n_in_from_ctl ? *(volatile unsigned long long*)&P.ctl->n_in : P.n_in;
     const uint32_t lt_mask = (1u << lane) - 1u;
 
     for (;; ++iteration) {
@@ -599,15 +615,20 @@ __global__ void __launch_bounds__(T) dfs_kernel(BtLaunch P)
             unsigned long long base = 0;
             if (lane == leader) base = atomicAdd(P.cursor, (unsigned long long)__popc(needmask));
             base = __shfl_sync(kFull, base, leader);
-            if (base + __popc(needmask) >= P.n_in) drained = true;
+            if (base + __popc(needmask) >= n_in) drained = true;
             if (need) {
                 const uint64_t my = base + __popc(needmask & lt_mask);
-                if (my < P.n_in && !*(volatile int*)P.abort_flag) {
+                if (my < n_in) {
                     const uint32_t* rec = P.in_rec + my * P.rec_words;
-                    if (!((rec[3] >> 17) & 1u)) {
-                        load_record<SM, T>(P, s, rec, stk, av, spill);
-                        if (P.stop_at_first && s.orig > *(volatile unsigned long long*)&P.first_item[s.pz])
-                            s.active = false;  // a lower subtree of this puzzle holds a solution
+                    const uint32_t flags = rec[3];
+                    if (!((flags >> 17) & 1u)) {
+                        if (*(volatile int*)P.abort_flag) {
+                            P.incomplete[flags & 0xFFFFu] = 1u;  // stopped: the record stays unsearched
+                        } else {
+                            load_record<SM, T>(P, s, rec, stk, av, spill);
+                            if (P.stop_at_first && s.orig > *(volatile unsigned long long*)&P.first_item[s.pz])
+                                s.active = false;  // a lower subtree of this puzzle holds a solution
+                        }
                     }
                 } else {
                     alive = false;
@@ -618,7 +639,7 @@ __global__ void __launch_bounds__(T) dfs_kernel(BtLaunch P)
             unsigned long long c = 0;
             if (lane == 0) c = *(volatile unsigned long long*)P.cursor;
             c = __shfl_sync(kFull, c, 0);
-            drained = c >= P.n_in;
+            drained = c >= n_in;
         }
         if (!__any_sync(kFull, alive)) break;
 
@@ -664,9 +685,11 @@ __global__ void __launch_bounds__(T) dfs_kernel(BtLaunch P)
                 account(P, s);
                 s.active = false;
                 if (stop) {
+                    // the lane stays alive: it goes on taking records only to mark
+                    // their puzzles incomplete, so every dropped piece of work is known
+                    P.incomplete[s.pz] = 1u;
                     atomicExch(P.abort_flag, 1);
                     atomicOr(P.status, EMP_DEV_ABORTED);
-                    alive = false;
                 } else {
                     atomicOr(P.status, EMP_DEV_SUPERSEDED);
                 }
@@ -681,8 +704,14 @@ __global__ void reset_kernel(BtLaunch P, uint32_t n_puzzles)
     if (i == 0) {
         P.abort_flag[0] = 0;
         P.status[0] = 0;
+        P.ctl->deadline = P.timeout_ns ? global_ns() + P.timeout_ns : 0ull;
+        P.ctl->n_in = 0;
+        P.ctl->rounds = 0;
+        P.ctl->records_in = P.n_in;
+        P.ctl->records_out = 0;
     }
     if (i < n_puzzles) {
+        P.incomplete[i] = 0;
         P.totals[2 * i] = 0;
         P.totals[2 * i + 1] = 0;
         P.first_item[i] = ~0ull;
@@ -695,7 +724,7 @@ __global__ void reset_kernel(BtLaunch P, uint32_t n_puzzles)
 // Initial records from split-depth prefixes (a strided selection of them).
 __global__ void make_records(const uint16_t* __restrict__ prefixes, const uint32_t* __restrict__ prefix_puzzle,
                              uint32_t depth, uint64_t first, uint64_t stride, uint64_t count, uint32_t rec_words,
-                             uint32_t* __restrict__ rec)
+                             uint32_t* __restrict__ rec, const uint32_t* __restrict__ puzzle_depth)
 {
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < count;
          i += (uint64_t)gridDim.x * blockDim.x) {
@@ -703,11 +732,41 @@ __global__ void make_records(const uint16_t* __restrict__ prefixes, const uint32
         uint32_t* r = rec + i * rec_words;
         r[0] = static_cast<uint32_t>(i);
         r[1] = static_cast<uint32_t>(i >> 32);
-        r[2] = depth;
-        r[3] = prefix_puzzle[j];
+        const uint32_t pz = prefix_puzzle[j];
+        const uint32_t len = puzzle_depth ? puzzle_depth[pz] : depth;
+        r[2] = len;
+        r[3] = pz;
         const uint16_t* p = prefixes + j * depth;
-        for (uint32_t l = 0; l < depth; l += 2) r[4 + (l >> 1)] = p[l] | (l + 1 < depth ? (uint32_t)p[l + 1] << 16 : 0u);
+        for (uint32_t l = 0; l < len; l += 2) r[4 + (l >> 1)] = p[l] | (l + 1 < len ? (uint32_t)p[l + 1] << 16 : 0u);
     }
+}
+
+// Graph runs: turns the records handed back by the round that just ended into
+// the next round's input and decides whether the loop goes on.
+__global__ void round_advance_kernel(BtLaunch P, cudaGraphConditionalHandle loop, uint32_t max_rounds)
+{
+    BtRunCtl* c = P.ctl;
+    const unsigned long long tail = *P.out_tail;
+    const unsigned long long n = tail < P.out_capacity ? tail : P.out_capacity;
+    c->rounds += 1;
+    c->records_out += n;
+    c->records_in += n;
+    c->n_in = n;
+    *P.cursor = 0;
+    *P.out_tail = 0;
+    cudaGraphSetConditional(loop, (n && c->rounds < max_rounds) ? 1u : 0u);
+}
+
+// Graph runs: copies the round's input records (ctl->n_in of them) to the input queue.
+__global__ void round_copy_kernel(BtLaunch P, uint4* __restrict__ dst, const uint4* __restrict__ src)
+{
+    const uint64_t words = *(volatile unsigned long long*)&P.ctl->n_in * P.rec_words;
+    const uint64_t vec = words / 4;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < vec; i += (uint64_t)gridDim.x * blockDim.x)
+        dst[i] = src[i];
+    const uint64_t tail = vec * 4 + blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (tail < words)
+        reinterpret_cast<uint32_t*>(dst)[tail] = reinterpret_cast<const uint32_t*>(src)[tail];
 }
 
 // Prefix (transitions) of selected subtree `i`, for the host.
@@ -715,7 +774,7 @@ __global__ void record_prefix(const uint32_t* __restrict__ rec, uint32_t rec_wor
 {
     const uint32_t* r = rec + i * rec_words;
     const uint32_t len = r[2] & 0xFFFFu;
-    for (uint32_t l = threadIdx.x; l < len; l += blockDim.x) out[l] = static_cast<uint16_t>(rec_t(r, l));
+    for (uint32_t l = threadIdx.x; l < 256; l += blockDim.x) out[l] = l < len ? static_cast<uint16_t>(rec_t(r, l)) : 0xFFFFu;
 }
 
 template <int KW, int T>
@@ -766,7 +825,37 @@ cudaError_t launch_expand(const BtLaunch& P, const uint16_t* parents, const uint
     const uint64_t blocks = std::min<uint64_t>((n_parents + threads - 1) / threads, 148ull * 64);
     expand_kernel<<<(unsigned)blocks, threads, 0, stream>>>(P, parents, parent_puzzle, n_parents, level, counts,
                                                             offsets, children, child_puzzle, level_nodes,
-                                                            level_sols, mode);
+                                                            level_sols, mode, nullptr);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_expand_frozen(const BtLaunch& P, const uint16_t* parents, const uint32_t* parent_puzzle,
+                                 uint64_t n_parents, uint32_t level, uint32_t* counts, const uint64_t* offsets,
+                                 uint16_t* children, uint32_t* child_puzzle, unsigned long long* level_nodes,
+                                 unsigned long long* level_sols, int mode, const uint8_t* frozen,
+                                 cudaStream_t stream)
+{
+    if (!n_parents) return cudaSuccess;
+    const uint32_t threads = 128;
+    const uint64_t blocks = std::min<uint64_t>((n_parents + threads - 1) / threads, 148ull * 64);
+    expand_kernel<<<(unsigned)blocks, threads, 0, stream>>>(P, parents, parent_puzzle, n_parents, level, counts,
+                                                            offsets, children, child_puzzle, level_nodes,
+                                                            level_sols, mode, frozen);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_round_advance(const BtLaunch& P, cudaGraphConditionalHandle loop, uint32_t max_rounds,
+                                 cudaStream_t stream)
+{
+    round_advance_kernel<<<1, 1, 0, stream>>>(P, loop, max_rounds);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_round_copy(const BtLaunch& P, uint32_t* dst, const uint32_t* src, cudaStream_t stream)
+{
+    // queues are allocated by cudaMalloc (256-byte aligned): 16-byte vector copies
+    round_copy_kernel<<<148 * 4, 256, 0, stream>>>(P, reinterpret_cast<uint4*>(dst),
+                                                   reinterpret_cast<const uint4*>(src));
     return cudaGetLastError();
 }
 
@@ -813,12 +902,12 @@ cudaError_t launch_bt_reset(const BtLaunch& P, uint32_t n_puzzles, cudaStream_t 
 
 cudaError_t launch_make_records(const uint16_t* prefixes, const uint32_t* prefix_puzzle, uint32_t depth,
                                 uint64_t first, uint64_t stride, uint64_t count, uint32_t rec_words, uint32_t* rec,
-                                cudaStream_t stream)
+                                cudaStream_t stream, const uint32_t* puzzle_depth)
 {
     if (!count) return cudaSuccess;
     const uint64_t blocks = std::min<uint64_t>((count + 255) / 256, 148ull * 32);
     make_records<<<(unsigned)blocks, 256, 0, stream>>>(prefixes, prefix_puzzle, depth, first, stride, count,
-                                                       rec_words, rec);
+                                                       rec_words, rec, puzzle_depth);
     return cudaGetLastError();
 }
 

@@ -24,6 +24,15 @@ struct FirstRecord {
     uint16_t t[256];        // transition per level
 };
 
+// Run state on the device, shared by the launches of one run.
+struct BtRunCtl {
+    unsigned long long deadline;     // absolute %globaltimer deadline of the run; 0 = none
+    unsigned long long n_in;         // graph runs: records of the current round
+    unsigned long long rounds;       // graph runs: DFS rounds launched
+    unsigned long long records_in;   // graph runs: records read by all rounds
+    unsigned long long records_out;  // graph runs: records handed back for a next round
+};
+
 struct BtLaunch {
     const uint32_t* tables = nullptr;         // all puzzle blobs
     const uint64_t* puzzle_offset = nullptr;  // word offset of each puzzle blob
@@ -52,6 +61,9 @@ struct BtLaunch {
     int* abort_flag = nullptr;                // set by the host or by a stopping thread
     int* status = nullptr;
     int stop_at_first = 0;
+    BtRunCtl* ctl = nullptr;                  // deadline; in graph runs also the round's record count
+    int n_in_from_ctl = 0;                    // 1: read the round's record count from ctl->n_in
+    uint32_t* incomplete = nullptr;           // per puzzle: 1 when some of its work was dropped (deadline, abort)
 };
 
 cudaError_t launch_expand(const BtLaunch& P, const uint16_t* parents, const uint32_t* parent_puzzle,
@@ -65,9 +77,24 @@ size_t dfs_smem_bytes(uint32_t max_levels, uint32_t max_avail_words, uint32_t th
 uint32_t record_words(uint32_t max_levels, uint32_t max_kw);
 cudaError_t launch_dfs(const BtLaunch& P, uint32_t blocks, uint32_t threads, cudaStream_t stream);
 cudaError_t launch_bt_reset(const BtLaunch& P, uint32_t n_puzzles, cudaStream_t stream);
+// frozen (per puzzle, may be null): puzzles whose prefixes are carried to the next
+// level unchanged (a 0xFFFF pad), neither expanded nor counted
+cudaError_t launch_expand_frozen(const BtLaunch& P, const uint16_t* parents, const uint32_t* parent_puzzle,
+                                 uint64_t n_parents, uint32_t level, uint32_t* counts, const uint64_t* offsets,
+                                 uint16_t* children, uint32_t* child_puzzle, unsigned long long* level_nodes,
+                                 unsigned long long* level_sols, int mode, const uint8_t* frozen,
+                                 cudaStream_t stream);
+// puzzle_depth (per puzzle, may be null): prefix length of each puzzle's records;
+// null = depth for all
 cudaError_t launch_make_records(const uint16_t* prefixes, const uint32_t* prefix_puzzle, uint32_t depth,
                                 uint64_t first, uint64_t stride, uint64_t count, uint32_t rec_words, uint32_t* rec,
-                                cudaStream_t stream);
+                                cudaStream_t stream, const uint32_t* puzzle_depth = nullptr);
+// Graph runs: the round controller (one thread) that turns this round's handed-back
+// records into the next round's input and sets the loop condition, and the copy of
+// those records into the input queue.
+cudaError_t launch_round_advance(const BtLaunch& P, cudaGraphConditionalHandle loop, uint32_t max_rounds,
+                                 cudaStream_t stream);
+cudaError_t launch_round_copy(const BtLaunch& P, uint32_t* dst, const uint32_t* src, cudaStream_t stream);
 cudaError_t launch_record_prefix(const uint32_t* rec, uint32_t rec_words, uint64_t i, uint16_t* out,
                                  cudaStream_t stream);
 const void* dfs_kernel_symbol(uint32_t max_kw, bool smem_tables, uint32_t threads);

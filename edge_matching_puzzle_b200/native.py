@@ -55,7 +55,9 @@ class BtConfig(ctypes.Structure):
         ("sample_stride", ctypes.c_uint32),
         ("sample_first", ctypes.c_uint32),
         ("table_placement", ctypes.c_uint32),
-        ("reserved", ctypes.c_uint32 * 3),
+        ("split_subtrees", ctypes.c_uint32),
+        ("use_graph", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32 * 1),
     ]
 
 
@@ -76,6 +78,16 @@ class BtResult(ctypes.Structure):
         ("dfs_busy_ms", ctypes.c_double),
         ("work_records", ctypes.c_uint64),
         ("handed_back", ctypes.c_uint64),
+    ]
+
+
+class TuneResult(ctypes.Structure):
+    _fields_ = [
+        ("best", BtConfig),
+        ("best_rate", ctypes.c_double),
+        ("default_rate", ctypes.c_double),
+        ("trials", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32),
     ]
 
 
@@ -123,6 +135,8 @@ SIGNATURES = {
     "emp_bt_plan_subtree_counts": (ctypes.c_int32, [ctypes.c_void_p, u64p, u64p, ctypes.c_uint64]),
     "emp_bt_plan_subtree_prefix": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_uint64, u16p, ctypes.c_uint32]),
     "emp_bt_plan_destroy": (None, [ctypes.c_void_p]),
+    "emp_bt_autotune": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_uint32, ctypes.POINTER(BtConfig), ctypes.c_uint32,
+                                         ctypes.POINTER(TuneResult)]),
     "emp_glutton_max": (ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(GmConfig), ctypes.POINTER(GmResult)]),
     "emp_glutton_max_noalloc": (ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(GmConfig), ctypes.POINTER(GmResult)]),
 }
@@ -223,6 +237,20 @@ def bt_count_batch(puzzles: Sequence[NativePuzzle], **kw) -> List[BtResult]:
     cfg = bt_config(**kw)
     check(load().emp_bt_count_batch(arr, len(puzzles), ctypes.byref(cfg), res))
     return list(res)
+
+
+def bt_autotune(puzzles: Sequence[NativePuzzle], trial_ms: int = 200, **kw) -> TuneResult:
+    """emp_bt_autotune: the fastest launch parameters for these puzzles (timed trials)."""
+    arr = (ctypes.c_void_p * len(puzzles))(*[p.handle for p in puzzles])
+    cfg = bt_config(**kw)
+    out = TuneResult()
+    check(load().emp_bt_autotune(arr, len(puzzles), ctypes.byref(cfg), trial_ms, ctypes.byref(out)))
+    return out
+
+
+def config_dict(cfg: BtConfig) -> dict:
+    return {name: (list(getattr(cfg, name)) if name == "reserved" else getattr(cfg, name))
+            for name, _ in BtConfig._fields_}
 
 
 def glutton_max(puzzle: NativePuzzle, push_budget: int = 0, timeout_ms: int = 0, device: int = -1) -> GmResult:

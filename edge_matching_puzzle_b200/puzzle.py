@@ -167,3 +167,18 @@ def board_string(width: int, height: int, cells: Sequence[int]) -> str:
         else:
             out.append(f"{(c >> 2) + 1:>{wd - 1}d}{'NESW'[c & 3]}")
     return "".join(out)
+
+
+def mixed_batch(count: int = 4096, seed: int = 2) -> List[Puzzle]:
+    """The batched workload: ``count`` square puzzles whose side is drawn uniformly from
+    4..9, border colours from 3..5 and interior colours from 4..10.  Instance i takes
+    four draws of one splitmix64 stream seeded with ``seed``: side, border colours,
+    interior colours and the generator seed of the puzzle."""
+    sm = SplitMix64(seed)
+    out = []
+    for _ in range(count):
+        side = 4 + sm.below(6)
+        border = 3 + sm.below(3)
+        interior = 4 + sm.below(7)
+        out.append(generate(side, side, border, interior, sm.next()))
+    return out

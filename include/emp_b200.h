@@ -102,7 +102,7 @@ typedef struct emp_bt_config {
     uint32_t blocks_per_sm;      /* 0 = as many as fit */
     uint32_t stop_at_first;      /* 1: stop once the reference's first solution is known */
     uint64_t reserved_budget;    /* unused, keep 0 */
-    uint32_t timeout_ms;         /* kernel deadline; 0 = none */
+    uint32_t timeout_ms;         /* deadline of a whole run (all rounds), on the device clock; 0 = none */
     int32_t device;              /* CUDA device ordinal; -1 = current device */
     uint32_t keep_subtree_counts;/* 1: keep per-subtree counts for emp_bt_plan_subtree_counts */
     uint32_t split_budget;       /* once a round's queue is empty, a thread that spent this many
@@ -113,7 +113,14 @@ typedef struct emp_bt_config {
     uint32_t sample_first;
     uint32_t table_placement;    /* 0 = auto (shared memory for a single puzzle), 1 = global memory,
                                     2 = shared memory (single puzzle only) */
-    uint32_t reserved[3];
+    uint32_t split_subtrees;     /* 0 = every puzzle is split at split_depth.  Otherwise each puzzle is
+                                    split at its own depth: the first level at which it has at least
+                                    this many subtrees, at most split_depth (0: no limit) and below
+                                    its piece count.  For batches of puzzles of mixed sizes. */
+    uint32_t use_graph;          /* 1: emp_bt_plan_run launches the whole run as one CUDA graph whose
+                                    device-side loop (a conditional node) starts each next round;
+                                    0: the host starts each round */
+    uint32_t reserved[1];
 } emp_bt_config;
 
 typedef struct emp_bt_result {
@@ -121,8 +128,9 @@ typedef struct emp_bt_result {
     uint64_t nodes;              /* "Total situations explored" (:412) */
     uint64_t subtrees;           /* prefixes at the split depth */
     uint64_t expansion_nodes;    /* placements at levels below the split depth */
-    int32_t status;              /* EMP_OK or EMP_INCOMPLETE */
-    uint32_t split_depth;
+    int32_t status;              /* EMP_OK, or EMP_INCOMPLETE when part of this puzzle's search was
+                                    dropped (deadline or cancel): its counts are then partial */
+    uint32_t split_depth;        /* this puzzle's split depth */
     uint32_t has_first_solution;
     uint32_t first_solution[256];/* per board position y*w+x: (piece id-1)<<2 | orientation */
     double kernel_ms;            /* DFS kernel time (device events, all rounds) */
@@ -165,6 +173,30 @@ emp_status emp_bt_plan_subtree_counts(emp_bt_plan plan, uint64_t *nodes, uint64_
 /* Prefix (split_depth transitions t = kind_index<<2|orientation) of a selected subtree. */
 emp_status emp_bt_plan_subtree_prefix(emp_bt_plan plan, uint64_t index, uint16_t *prefix, uint32_t capacity);
 void emp_bt_plan_destroy(emp_bt_plan plan);
+
+/* ---------------- autotuner (no counterpart in the reference) ---------------- */
+
+typedef struct emp_bt_tune_result {
+    emp_bt_config best;          /* base configuration with the tuned fields of the fastest trial */
+    double best_rate;            /* its placements per second of device time */
+    double default_rate;         /* the first trial's rate (base configuration, library defaults) */
+    uint32_t trials;             /* configurations timed */
+    uint32_t reserved;
+} emp_bt_tune_result;
+
+/* Chooses the launch parameters for a set of puzzles by timing short runs on the
+ * device.  Starting from base (NULL = defaults), it tunes one field at a time, keeping
+ * each field's fastest value before moving on:
+ *   threads_per_block   64, 128, 256
+ *   split_subtrees      per-puzzle split targets (batches of several puzzles) or
+ *   split_depth         split depths (a single puzzle)
+ *   split_budget        steps before a thread hands work back
+ *   table_placement     shared or global memory (a single puzzle)
+ * Every trial builds a plan (upload and prefix expansion, not timed) and runs it with
+ * a deadline of trial_ms; its rate is the placements counted divided by the run's
+ * device time. */
+emp_status emp_bt_autotune(const emp_puzzle *puzzles, uint32_t count, const emp_bt_config *base,
+                           uint32_t trial_ms, emp_bt_tune_result *out);
 
 /* ---------------- glutton max search (CUDA_glutton_max semantics) ---------------- */
 
