@@ -42,6 +42,8 @@ UNIT = "placements/s"
 WORKLOAD = (f"exhaustive row-major count of 16 seeded {WIDTH}x{HEIGHT} puzzles ({BORDER} border / {INTERIOR} interior "
             f"colours, seeds 0..15), split depth {DEPTH}, one step = 1/{SLICES} slice of the depth-{DEPTH} subtrees")
 L2_BYTES = 126 * 1024 * 1024
+# DRAM bytes (read + write) of one dfs_kernel round on this workload, from one ncu capture
+DFS_LAUNCH_DRAM_BYTES = 172.6e6
 
 
 def env_int(name, default):
@@ -528,7 +530,11 @@ def main():
             "gpu_launches": launches,
             "roofline": {"bound": "hbm", "achieved": dram_alg / (launch_ms / 1000) / 1e9,
                          "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                         "frac": dram_alg / (launch_ms / 1000) / 1e9 / peaks["hbm_gbs"], "traffic": None,
+                         "frac": dram_alg / (launch_ms / 1000) / 1e9 / peaks["hbm_gbs"],
+                         "traffic": DFS_LAUNCH_DRAM_BYTES,
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one dfs_kernel round "
+                                           "(seed-0 slice, same grid and table staging; caches flushed by ncu), "
+                                           "profiles/dfs_kernel_8x8_seed0_ncu_full.md",
                          "peak_source": peak_kind,
                          "note": "dfs_kernel keeps its state on chip; DRAM only carries work records, so the "
                                  "on-chip roofline below is the binding one"},
