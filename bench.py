@@ -32,6 +32,8 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+from edge_matching_puzzle_b200.sharding import items_for_rank, reduce_time_and_counts, slice_for_step  # noqa: E402
+
 WIDTH, HEIGHT, BORDER, INTERIOR = 8, 8, 4, 8
 SEEDS = list(range(16))
 DEPTH = 12
@@ -218,7 +220,7 @@ def run_batch(args, rank, world, local_rank):
         torch.cuda.synchronize()
 
     batch = mixed_batch(BATCH_COUNT)
-    mine = batch[rank::world]  # instances shard across ranks: no data-path collective
+    mine = items_for_rank(batch, rank, world)  # instances shard across ranks: no data-path collective
     handles = [native.NativePuzzle(p.width, p.height, p.colors) for p in mine]
     tune = native.bt_autotune(handles, trial_ms=400, use_graph=1, table_placement=1, device=local_rank)
     cfg = native.config_dict(tune.best)
@@ -274,12 +276,9 @@ def run_batch(args, rank, world, local_rank):
             d2h = len(hp) * (16 + 8 + 4 + 528)
         for p in hp:
             p.close()
-    if dist is not None:
-        t = torch.tensor([ms, float(nodes), e_sec, float(e_nodes), float(complete)], dtype=torch.float64, device="cuda")
-        mx = t.clone()
-        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
-        dist.all_reduce(t, op=dist.ReduceOp.SUM)
-        ms, nodes, e_sec, e_nodes, complete = mx[0].item(), t[1].item(), mx[2].item(), t[3].item(), int(t[4].item())
+    ms, (nodes, e_nodes, complete) = reduce_time_and_counts(dist, "cuda", ms, [float(nodes), float(e_nodes), float(complete)])
+    e_sec, _ = reduce_time_and_counts(dist, "cuda", e_sec, [])
+    complete = int(complete)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         threads = os.cpu_count() or 1
@@ -314,6 +313,85 @@ def run_batch(args, rank, world, local_rank):
     plan.close()
     if dist is not None:
         dist.destroy_process_group()
+
+
+GM_SIDE, GM_BORDER, GM_INTERIOR, GM_SEED = 16, 5, 17, 7
+GM_STEP_MS = 10000
+GM_CPU_BUDGET = 100_000
+GM_WORKLOAD = (f"glutton max search of the seeded {GM_SIDE}x{GM_SIDE} puzzle ({GM_BORDER} border / {GM_INTERIOR} "
+               f"interior colours, seed {GM_SEED}); one step = the search from the empty board for {GM_STEP_MS} ms of "
+               f"device time (or the placement budget); placements = candidate trial evaluations + committed "
+               f"placements")
+
+
+def run_glutton(args, rank, world, local_rank):
+    """Greedy max-placement search of the 16x16 puzzle: placements/s of one search."""
+    import torch
+    from edge_matching_puzzle_b200 import native
+    from edge_matching_puzzle_b200.puzzle import generate
+    torch.cuda.set_device(local_rank)
+    if rank != 0:
+        return  # one search: replicas would repeat the same trajectory
+    pz = generate(GM_SIDE, GM_SIDE, GM_BORDER, GM_INTERIOR, GM_SEED)
+    handle = native.NativePuzzle(pz.width, pz.height, pz.colors)
+    budget = args.gm_budget
+    sampler = ClockSampler(torch.cuda.current_device())
+    placements = 0
+    sec = 0.0
+    res = None
+    for i in range(args.warmup + args.steps):
+        if i == args.warmup:
+            sampler.__enter__()
+        torch.cuda.synchronize()
+        r = native.glutton_max(handle, timeout_ms=GM_STEP_MS if not budget else 0, placement_budget=budget,
+                               device=local_rank)
+        if i >= args.warmup:
+            placements += r.trials + r.pushes
+            sec += r.kernel_ms / 1000.0
+            res = r
+    sampler.__exit__()
+    clocks = sampler.summary()
+    # end to end: the public call from host colours (puzzle tables built and uploaded inside)
+    t0 = time.perf_counter()
+    h2 = native.NativePuzzle(pz.width, pz.height, pz.colors)
+    er = native.glutton_max(h2, timeout_ms=GM_STEP_MS if not budget else 0, placement_budget=budget, device=local_rank)
+    e_sec = time.perf_counter() - t0
+    h2.close()
+    cpu = None
+    if not args.no_cpu:
+        from oracle.oracle import OraclePuzzle
+        op = OraclePuzzle(pz.width, pz.height, pz.colors)
+        t1 = time.perf_counter()
+        cr = op.glutton(budget=GM_CPU_BUDGET)
+        csec = time.perf_counter() - t1
+        cpu = {"value": cr.placements / csec, "unit": UNIT, "cores": 1, "kind": "port",
+               "sample": f"the first {GM_CPU_BUDGET} placements of the same search (level 0), CPU oracle "
+                         f"(restatement of the reference's glutton kernel, one thread)"}
+    value = placements / sec
+    n = GM_SIDE * GM_SIDE
+    peak_sm = 4 * 32 * ((clocks or {}).get("sm_max_mhz") or 1965.0) * 1e6  # lane-ops/s of one SM
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000 * sec / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u32", "data": "synthetic",
+        "config": {"workload": GM_WORKLOAD, "placement_budget": budget or None, "blocks": 1, "threads": 1024,
+                   "l2": "the search state lives in shared memory; inputs (tables) are read once per level"},
+        "gpu_launches": args.steps,
+        "best_level": res.max_level, "final_level": res.level, "status": res.status,
+        "levels_per_s": res.levels / (res.kernel_ms / 1000.0), "pushes": res.pushes, "pops": res.pops,
+        "passes": res.passes,
+        "roofline_onchip": {
+            "kernel": "gm_kernel (one block of 1024 threads on one SM)",
+            "int_issue_peak_one_sm_lane_ops": peak_sm,
+            "note": "a trial only rescans the free positions whose colour constraints it changes, so the "
+                    "reference's per-trial work 32*(26L+3c+31) lane-ops is an upper bound of the work done",
+        },
+        "clocks": clocks,
+        "e2e": {"value": (er.trials + er.pushes) / e_sec, "unit": UNIT, "h2d_bytes_per_step": 4 * n + 4200,
+                "d2h_bytes_per_step": 4200},
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(out), flush=True)
 
 
 def run_reference(args, rank, world):
@@ -351,8 +429,11 @@ def main():
     ap.add_argument("--full", action="store_true", help="run all slices (the complete count) and print per-seed totals")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
-    ap.add_argument("--workload", default="exhaustive", choices=["exhaustive", "batch"],
-                    help="exhaustive: the 16 seeded 8x8 puzzles (default); batch: 4096 mixed instances")
+    ap.add_argument("--workload", default="exhaustive", choices=["exhaustive", "batch", "glutton"],
+                    help="exhaustive: the 16 seeded 8x8 puzzles (default); batch: 4096 mixed instances; "
+                         "glutton: the 16x16 glutton max search")
+    ap.add_argument("--gm-budget", type=int, default=0,
+                    help="glutton: placement budget of each search (0: a time-bounded step)")
     ap.add_argument("--counts-out", default=None, help="batch: write per-instance counts (JSON lines) here")
     ap.add_argument("--seeds", default=None,
                     help="comma-separated subset of the workload seeds (a smaller case for profiling)")
@@ -370,6 +451,9 @@ def main():
         return
     if args.workload == "batch":
         run_batch(args, rank, world, local_rank)
+        return
+    if args.workload == "glutton":
+        run_glutton(args, rank, world, local_rank)
         return
 
     import torch
@@ -438,7 +522,7 @@ def main():
     dev_index = torch.cuda.current_device()
     sampler = ClockSampler(dev_index)
     for i in range(args.warmup + args.steps):
-        s = (i * world + rank) % SLICES
+        s = slice_for_step(i, rank, world, SLICES)
         if i == args.warmup:
             sampler.__enter__()
         flush.add_(1)  # writes 252 MB: evicts L2 between steps
@@ -458,14 +542,7 @@ def main():
             launches += sum(2 + r.rounds for r in res)  # make_records + reset + one DFS launch per round
     sampler.__exit__()
     clocks = sampler.summary()
-    if dist is not None:
-        t = torch.tensor([ms, float(nodes)], dtype=torch.float64, device="cuda")
-        mx = t.clone()
-        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
-        dist.all_reduce(t, op=dist.ReduceOp.SUM)
-        ms_max, nodes_all = mx[0].item(), t[1].item()
-    else:
-        ms_max, nodes_all = ms, float(nodes)
+    ms_max, (nodes_all,) = reduce_time_and_counts(dist, "cuda", ms, [float(nodes)])
     value = nodes_all / (ms_max / 1000.0)
 
     # ---------------- end to end through the public one-shot call ----------------
@@ -477,7 +554,7 @@ def main():
         e_sec = 0.0
         h2d = d2h = 0
         for i in range(1 + args.steps):
-            s = ((args.warmup - 1 + i) * world + rank) % SLICES  # the timed steps use the value leg's slices
+            s = slice_for_step(args.warmup - 1 + i, rank, world, SLICES)  # the value leg's timed slices
             barrier()
             t0 = time.perf_counter()
             hp = [native.NativePuzzle(WIDTH, HEIGHT, p.colors) for p in host_inputs]
@@ -493,12 +570,7 @@ def main():
                 d2h = (8 * (2 * len(hp) + DEPTH + res[0].rounds) + 528 * len(hp) + 8)
             for p in hp:
                 p.close()
-        if dist is not None:
-            t = torch.tensor([e_sec, float(e_nodes)], dtype=torch.float64, device="cuda")
-            mx = t.clone()
-            dist.all_reduce(mx, op=dist.ReduceOp.MAX)
-            dist.all_reduce(t, op=dist.ReduceOp.SUM)
-            e_sec, e_nodes = mx[0].item(), t[1].item()
+        e_sec, (e_nodes,) = reduce_time_and_counts(dist, "cuda", e_sec, [float(e_nodes)])
         e2e = {"value": e_nodes / e_sec, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h}
 
     # ---------------- CPU baseline (oracle) and algorithmic work ----------------

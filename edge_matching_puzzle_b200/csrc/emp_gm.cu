@@ -351,7 +351,10 @@ __global__ void __launch_bounds__(kThreads, 1) gm_kernel(GmLaunch P)
         const uint32_t level = sm.level;
         if (level >= S) break;  // full board (level == S) or exhausted (wrapped below 0)
         if (tid == 0) {
-            if ((P.push_budget && st->pushes >= P.push_budget) || (deadline && global_ns() > deadline)) sm.stop = 1;
+            if ((P.push_budget && st->pushes >= P.push_budget) ||
+                (P.placement_budget && st->trials + st->pushes >= P.placement_budget) ||
+                (deadline && global_ns() > deadline))
+                sm.stop = 1;
         }
         __syncthreads();
         if (sm.stop) break;

@@ -34,6 +34,7 @@ struct GmLaunch {
     GmState* state;
     uint32_t n, width, ncolours;
     unsigned long long push_budget;   // stop after this many pushes (0: none)
+    unsigned long long placement_budget;  // stop once trials + pushes reach this (0: none)
     unsigned long long timeout_ns;    // stop after this long (0: none)
 };
 

@@ -133,6 +133,7 @@ extern "C" emp_status emp_glutton_max(emp_puzzle puzzle, const emp_gm_config* co
     P.width = m.width;
     P.ncolours = m.border_id;
     P.push_budget = cfg.push_budget;
+    P.placement_budget = cfg.placement_budget;
     // without a caller limit the search still stops after an hour on the device
     const unsigned long long ms_limit = cfg.timeout_ms ? cfg.timeout_ms : 3600000ull;
     P.timeout_ns = ms_limit * 1000000ull;
@@ -272,6 +273,7 @@ extern "C" emp_status emp_glutton_max_noalloc(emp_puzzle puzzle, const emp_gm_co
     P.width = m.width;
     P.ncolours = m.border_id;
     P.push_budget = cfg.push_budget;
+    P.placement_budget = cfg.placement_budget;
     const unsigned long long ms_limit = cfg.timeout_ms ? cfg.timeout_ms : 3600000ull;
     P.timeout_ns = ms_limit * 1000000ull;
     // no CUDA events (they are driver objects to create and destroy): the time

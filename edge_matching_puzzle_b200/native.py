@@ -93,7 +93,7 @@ class TuneResult(ctypes.Structure):
 
 class GmConfig(ctypes.Structure):
     _fields_ = [("push_budget", ctypes.c_uint64), ("timeout_ms", ctypes.c_uint32), ("device", ctypes.c_int32),
-                ("reserved", ctypes.c_uint32 * 8)]
+                ("placement_budget", ctypes.c_uint64), ("reserved", ctypes.c_uint32 * 6)]
 
 
 class GmResult(ctypes.Structure):
@@ -253,9 +253,11 @@ def config_dict(cfg: BtConfig) -> dict:
             for name, _ in BtConfig._fields_}
 
 
-def glutton_max(puzzle: NativePuzzle, push_budget: int = 0, timeout_ms: int = 0, device: int = -1) -> GmResult:
+def glutton_max(puzzle: NativePuzzle, push_budget: int = 0, timeout_ms: int = 0, device: int = -1,
+                placement_budget: int = 0) -> GmResult:
     cfg = GmConfig()
     cfg.push_budget = push_budget
+    cfg.placement_budget = placement_budget
     cfg.timeout_ms = timeout_ms
     cfg.device = device
     r = GmResult()

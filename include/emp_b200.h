@@ -204,7 +204,10 @@ typedef struct emp_gm_config {
     uint64_t push_budget;        /* stop after this many committed placements; 0 = none */
     uint32_t timeout_ms;         /* stop after this long on the device; 0 = one hour */
     int32_t device;              /* CUDA device ordinal; -1 = current device */
-    uint32_t reserved[8];
+    uint64_t placement_budget;   /* stop at the first level that starts with at least this many
+                                    placements done (candidate trial evaluations + committed
+                                    placements, the kernel's own count); 0 = none */
+    uint32_t reserved[6];
 } emp_gm_config;
 
 typedef struct emp_gm_result {

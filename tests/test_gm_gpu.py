@@ -62,3 +62,21 @@ def test_random_puzzles_full_search(seed):
 def test_push_budget_trajectory(seed, budget):
     """Bounded searches on larger puzzles stop at the same point with the same best board."""
     _compare(generate(8, 8, 4, 8, seed), push_budget=budget)
+
+
+def test_placement_budget_stops_the_search():
+    """A placement budget (trial evaluations + pushes) stops the search at a level start."""
+    import ctypes
+    pz = generate(5, 5, 3, 5, 11)
+    h = native.NativePuzzle(5, 5, pz.colors)
+    full = native.glutton_max(h, timeout_ms=60000)
+    budget = (full.trials + full.pushes) // 2
+    cfg = native.GmConfig()
+    cfg.device = -1
+    cfg.timeout_ms = 60000
+    cfg.placement_budget = budget
+    r = native.GmResult()
+    st = native.load().emp_glutton_max(h.handle, ctypes.byref(cfg), ctypes.byref(r))
+    assert st == native.EMP_INCOMPLETE and r.status == 1
+    assert r.trials + r.pushes >= budget
+    assert r.levels < full.levels
