@@ -224,7 +224,7 @@ def run_batch(args, rank, world, local_rank):
     handles = [native.NativePuzzle(p.width, p.height, p.colors) for p in mine]
     tune = native.bt_autotune(handles, trial_ms=400, use_graph=1, table_placement=1, device=local_rank)
     cfg = native.config_dict(tune.best)
-    cfg.pop("reserved")
+
     cfg.update(timeout_ms=BATCH_STEP_MS, use_graph=1, device=local_rank)
     plan = native.BtPlan(handles, **cfg)
     flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.int32, device="cuda")

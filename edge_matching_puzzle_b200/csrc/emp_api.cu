@@ -163,6 +163,7 @@ struct emp_bt_plan_t {
         P.abort_flag = flags.as<int>();
         P.status = flags.as<int>() + 1;
         P.stop_at_first = cfg.stop_at_first ? 1 : 0;
+        P.stop_at_any = cfg.stop_at_any ? 1 : 0;
         P.ctl = ctl.as<emp::BtRunCtl>();
         P.incomplete = incomplete.as<uint32_t>();
         return P;
@@ -581,9 +582,13 @@ extern "C" emp_status emp_bt_plan_results(emp_bt_plan plan, emp_bt_result* resul
     std::vector<uint32_t> incomplete(P);
     CUDA_TRY(cudaMemcpy(incomplete.data(), plan->incomplete.p, sizeof(uint32_t) * P, cudaMemcpyDeviceToHost));
     (void)flags;
+    emp::BtRunCtl c{};
+    CUDA_TRY(cudaMemcpy(&c, plan->ctl.p, sizeof(c), cudaMemcpyDeviceToHost));
+    const uint32_t first_found_us =
+        c.first_found_ns ? static_cast<uint32_t>(std::min<unsigned long long>((c.first_found_ns - c.start_ns) / 1000,
+                                                                              0xFFFFFFFFull))
+                         : 0u;
     if (plan->graph_ran) {
-        emp::BtRunCtl c{};
-        CUDA_TRY(cudaMemcpy(&c, plan->ctl.p, sizeof(c), cudaMemcpyDeviceToHost));
         if (c.n_in) return fail(EMP_ERR_CUDA, "emp_bt_plan_results: the graph run stopped after too many rounds");
         plan->rounds = static_cast<uint32_t>(c.rounds);
         plan->records_in = c.records_in;
@@ -602,6 +607,7 @@ extern "C" emp_status emp_bt_plan_results(emp_bt_plan plan, emp_bt_result* resul
         r.status = incomplete[i] ? EMP_INCOMPLETE : EMP_OK;
         r.kernel_ms = ms;
         r.rounds = plan->rounds;
+        r.first_found_us = first_found_us;
         r.dfs_busy_ms = plan->busy_ms;
         r.work_records = plan->records_in;
         r.handed_back = plan->records_out;

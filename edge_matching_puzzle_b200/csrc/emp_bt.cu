@@ -649,7 +649,14 @@ __global__ void __launch_bounds__(T) dfs_kernel(BtLaunch P)
             if (s.active) {
                 bool solved = false;
                 if (dfs_step<KW, SM, T>(P, s, stk, av, spill, &solved)) {
-                    if (solved) record_solution<T>(P, s, stk);
+                    if (solved) {
+                        record_solution<T>(P, s, stk);
+                        if (P.stop_at_any) {
+                            // first solution of the run: note the time and stop every thread
+                            atomicCAS(&P.ctl->first_found_ns, 0ull, static_cast<unsigned long long>(global_ns()));
+                            atomicExch(P.abort_flag, 1);
+                        }
+                    }
                 } else {
                     account(P, s);
                     s.active = false;
@@ -704,7 +711,10 @@ __global__ void reset_kernel(BtLaunch P, uint32_t n_puzzles)
     if (i == 0) {
         P.abort_flag[0] = 0;
         P.status[0] = 0;
-        P.ctl->deadline = P.timeout_ns ? global_ns() + P.timeout_ns : 0ull;
+        const unsigned long long now = global_ns();
+        P.ctl->deadline = P.timeout_ns ? now + P.timeout_ns : 0ull;
+        P.ctl->start_ns = now;
+        P.ctl->first_found_ns = 0;
         P.ctl->n_in = 0;
         P.ctl->rounds = 0;
         P.ctl->records_in = P.n_in;

@@ -31,6 +31,8 @@ struct BtRunCtl {
     unsigned long long rounds;       // graph runs: DFS rounds launched
     unsigned long long records_in;   // graph runs: records read by all rounds
     unsigned long long records_out;  // graph runs: records handed back for a next round
+    unsigned long long start_ns;     // %globaltimer at the start of the run
+    unsigned long long first_found_ns;  // %globaltimer when the first solution was found (0: none)
 };
 
 struct BtLaunch {
@@ -61,6 +63,7 @@ struct BtLaunch {
     int* abort_flag = nullptr;                // set by the host or by a stopping thread
     int* status = nullptr;
     int stop_at_first = 0;
+    int stop_at_any = 0;                      // stop the whole run at the first solution found
     BtRunCtl* ctl = nullptr;                  // deadline; in graph runs also the round's record count
     int n_in_from_ctl = 0;                    // 1: read the round's record count from ctl->n_in
     uint32_t* incomplete = nullptr;           // per puzzle: 1 when some of its work was dropped (deadline, abort)

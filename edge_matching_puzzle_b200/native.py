@@ -57,7 +57,7 @@ class BtConfig(ctypes.Structure):
         ("table_placement", ctypes.c_uint32),
         ("split_subtrees", ctypes.c_uint32),
         ("use_graph", ctypes.c_uint32),
-        ("reserved", ctypes.c_uint32 * 1),
+        ("stop_at_any", ctypes.c_uint32),
     ]
 
 
@@ -74,7 +74,7 @@ class BtResult(ctypes.Structure):
         ("kernel_ms", ctypes.c_double),
         ("total_ms", ctypes.c_double),
         ("rounds", ctypes.c_uint32),
-        ("reserved", ctypes.c_uint32),
+        ("first_found_us", ctypes.c_uint32),
         ("dfs_busy_ms", ctypes.c_double),
         ("work_records", ctypes.c_uint64),
         ("handed_back", ctypes.c_uint64),
@@ -249,8 +249,7 @@ def bt_autotune(puzzles: Sequence[NativePuzzle], trial_ms: int = 200, **kw) -> T
 
 
 def config_dict(cfg: BtConfig) -> dict:
-    return {name: (list(getattr(cfg, name)) if name == "reserved" else getattr(cfg, name))
-            for name, _ in BtConfig._fields_}
+    return {name: getattr(cfg, name) for name, _ in BtConfig._fields_}
 
 
 def glutton_max(puzzle: NativePuzzle, push_budget: int = 0, timeout_ms: int = 0, device: int = -1,

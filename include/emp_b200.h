@@ -120,7 +120,8 @@ typedef struct emp_bt_config {
     uint32_t use_graph;          /* 1: emp_bt_plan_run launches the whole run as one CUDA graph whose
                                     device-side loop (a conditional node) starts each next round;
                                     0: the host starts each round */
-    uint32_t reserved[1];
+    uint32_t stop_at_any;        /* 1: stop the whole run at the first solution found by any thread
+                                    (time to a first solution; counts are then partial) */
 } emp_bt_config;
 
 typedef struct emp_bt_result {
@@ -136,7 +137,8 @@ typedef struct emp_bt_result {
     double kernel_ms;            /* DFS kernel time (device events, all rounds) */
     double total_ms;             /* whole call, host clock */
     uint32_t rounds;             /* DFS rounds (work handed back between rounds) */
-    uint32_t reserved;
+    uint32_t first_found_us;     /* device time from the start of the run to the first solution
+                                    found by any thread, in microseconds; 0 = none found */
     double dfs_busy_ms;          /* sum of the DFS launches' device times (no gaps between rounds) */
     uint64_t work_records;       /* work records read by the DFS launches (all rounds) */
     uint64_t handed_back;        /* work records written back for a next round */

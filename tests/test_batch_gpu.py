@@ -113,7 +113,7 @@ def test_autotune_picks_a_runnable_configuration():
     assert tune.trials >= 8
     assert tune.best_rate >= tune.default_rate > 0
     best = native.config_dict(tune.best)
-    best.pop("reserved")
+
     res = native.bt_count_batch(handles, **best)
     for pz, r in zip(puzzles, res):
         assert (r.nodes, r.solutions) == _oracle_counts(pz)

@@ -165,3 +165,22 @@ def test_timeout_stops_kernel():
     st = native.load().emp_bt_count(npz.handle, ctypes.byref(cfg), ctypes.byref(r))
     assert st == native.EMP_INCOMPLETE
     assert r.kernel_ms < 5000
+
+
+def test_stop_at_any_solution(config_counts):
+    """stop_at_any ends the run at the first solution any thread finds: a solution board,
+    a device time to it, fewer placements than the whole count.  A puzzle without
+    solutions is counted completely."""
+    recs = {r["seed"]: r for r in config_counts["records"] if r["config"] == "8x8"}
+    pz = generate(8, 8, 4, 8, 4)  # one solution
+    npz = native.NativePuzzle(8, 8, pz.colors)
+    full = native.bt_count(npz, split_depth=12)
+    r = native.bt_count(npz, split_depth=12, stop_at_any=1)
+    assert r.has_first_solution and r.first_found_us > 0
+    assert list(r.first_solution) == list(full.first_solution)
+    assert r.nodes < recs[4]["nodes"]
+    pz0 = generate(8, 8, 4, 8, 12)  # no solution
+    r0 = native.bt_count(native.NativePuzzle(8, 8, pz0.colors), split_depth=12, stop_at_any=1)
+    assert r0.first_found_us == 0 and not r0.has_first_solution
+    assert (r0.nodes, r0.solutions) == (recs[12]["nodes"], 0)
+    assert r0.status == native.EMP_OK
