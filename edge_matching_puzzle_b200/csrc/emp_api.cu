@@ -4,6 +4,7 @@
 #include "emp_bt.h"
 #include "emp_common.h"
 #include "emp_model.h"
+#include "emp_plan.h"
 
 #include <cuda_runtime.h>
 
@@ -90,85 +91,6 @@ extern "C" emp_status emp_puzzle_export_tables(emp_puzzle p, uint32_t* out, uint
 // ---------------------------------------------------------------------------
 // exhaustive backtracker plans
 
-struct emp_bt_plan_t {
-    std::vector<emp_puzzle> puzzles;
-    emp_bt_config cfg{};
-    int device = 0;
-    uint32_t depth = 0, max_levels = 0, max_avail = 0, max_kw = 0;
-    uint32_t threads = 128, blocks = 0, rec_words = 0, smem_tab_words = 0;
-    uint64_t capacity = 0, budget = 0;
-    DeviceBuffer tables, poff;
-    DeviceBuffer prefixes, prefix_puzzle;     // split-depth prefixes (all)
-    DeviceBuffer rec_init, rec_a, rec_b;      // initial records (selection), round queues
-    DeviceBuffer counters;                    // [0] cursor, [1] output tail
-    DeviceBuffer totals, first_item, records, flags, item_nodes, item_sols, spill, prefix_out;
-    DeviceBuffer ctl, incomplete, puzzle_depth_dev;
-    std::vector<uint32_t> puzzle_depth;       // per puzzle split depth
-    bool adaptive = false;                    // per puzzle split depths (split_subtrees)
-    cudaStream_t capture_stream = nullptr;    // graph runs: stream the graph is captured on
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t graph_exec = nullptr;
-    bool graph_ran = false;
-    uint64_t n_all = 0, n_init = 0;
-    bool sampled = false;
-    std::vector<unsigned long long> exp_nodes, exp_sols;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr, evr0 = nullptr, evr1 = nullptr;
-    bool ran = false;
-    uint32_t rounds = 0;
-    double busy_ms = 0;
-    uint64_t records_in = 0, records_out = 0;
-
-    void drop_graph()
-    {
-        if (graph_exec) cudaGraphExecDestroy(graph_exec);
-        if (graph) cudaGraphDestroy(graph);
-        graph_exec = nullptr;
-        graph = nullptr;
-    }
-
-    ~emp_bt_plan_t()
-    {
-        drop_graph();
-        if (capture_stream) cudaStreamDestroy(capture_stream);
-        if (ev0) cudaEventDestroy(ev0);
-        if (ev1) cudaEventDestroy(ev1);
-        if (evr0) cudaEventDestroy(evr0);
-        if (evr1) cudaEventDestroy(evr1);
-    }
-
-    emp::BtLaunch launch() const
-    {
-        emp::BtLaunch P;
-        P.tables = tables.as<uint32_t>();
-        P.puzzle_offset = poff.as<uint64_t>();
-        P.depth = depth;
-        P.max_levels = max_levels;
-        P.max_avail_words = max_avail;
-        P.max_kw = max_kw;
-        P.spill = spill.as<uint64_t>();
-        P.smem_tab_words = smem_tab_words;
-        P.rec_words = rec_words;
-        P.rec_r_off = rec_words - 2 * max_kw;
-        P.out_capacity = capacity;
-        P.item_budget = budget;
-        unsigned long long* c = counters.as<unsigned long long>();
-        P.cursor = c;
-        P.out_tail = c + 1;
-        P.totals = totals.as<unsigned long long>();
-        P.item_nodes = item_nodes.as<unsigned long long>();
-        P.item_sols = item_sols.as<unsigned long long>();
-        P.first_item = first_item.as<unsigned long long>();
-        P.first_records = records.as<emp::FirstRecord>();
-        P.timeout_ns = static_cast<unsigned long long>(cfg.timeout_ms) * 1000000ull;
-        P.abort_flag = flags.as<int>();
-        P.status = flags.as<int>() + 1;
-        P.stop_at_first = cfg.stop_at_first ? 1 : 0;
-        P.stop_at_any = cfg.stop_at_any ? 1 : 0;
-        P.ctl = ctl.as<emp::BtRunCtl>();
-        P.incomplete = incomplete.as<uint32_t>();
-        return P;
-    }
-};
 
 namespace {
 
@@ -288,8 +210,9 @@ emp_status expand(emp_bt_plan_t& pl)
     return EMP_OK;
 }
 
-// Initial records for subtrees first, first+stride, ... (count of them).
-emp_status build_initial(emp_bt_plan_t& pl, uint64_t first, uint64_t stride, uint64_t count)
+}  // namespace
+
+emp_status plan_build_initial(emp_bt_plan_t& pl, uint64_t first, uint64_t stride, uint64_t count)
 {
     CUDA_TRY(pl.rec_init.alloc(sizeof(uint32_t) * pl.rec_words * std::max<uint64_t>(count, 1)));
     CUDA_TRY(emp::launch_make_records(pl.prefixes.as<uint16_t>(), pl.prefix_puzzle.as<uint32_t>(), pl.depth, first,
@@ -303,8 +226,6 @@ emp_status build_initial(emp_bt_plan_t& pl, uint64_t first, uint64_t stride, uin
     pl.n_init = count;
     return EMP_OK;
 }
-
-}  // namespace
 
 extern "C" emp_status emp_bt_plan_create(const emp_puzzle* puzzles, uint32_t count, const emp_bt_config* config,
                                          emp_bt_plan* out)
@@ -403,7 +324,7 @@ extern "C" emp_status emp_bt_plan_create(const emp_puzzle* puzzles, uint32_t cou
     CUDA_TRY(pl->rec_a.alloc(sizeof(uint32_t) * pl->rec_words * pl->capacity));
     CUDA_TRY(pl->rec_b.alloc(sizeof(uint32_t) * pl->rec_words * pl->capacity));
     pl->budget = pl->cfg.split_budget ? pl->cfg.split_budget : 2048u;
-    EMP_TRY(build_initial(*pl, 0, 1, pl->n_all));
+    EMP_TRY(plan_build_initial(*pl, 0, 1, pl->n_all));
     *out = pl.release();
     return EMP_OK;
 }
@@ -424,7 +345,7 @@ extern "C" emp_status emp_bt_plan_select(emp_bt_plan plan, uint64_t first, uint6
         return fail(EMP_ERR_INVALID, "emp_bt_plan_select: selection past the last subtree");
     CUDA_TRY(cudaSetDevice(plan->device));
     plan->drop_graph();  // the graph holds the previous selection's records
-    EMP_TRY(build_initial(*plan, first, stride, count));
+    EMP_TRY(plan_build_initial(*plan, first, stride, count));
     plan->sampled = true;
     return EMP_OK;
 }

@@ -91,6 +91,22 @@ class TuneResult(ctypes.Structure):
     ]
 
 
+class MlpTrainConfig(ctypes.Structure):
+    _fields_ = [("epochs", ctypes.c_uint32), ("batch", ctypes.c_uint32), ("learning_rate", ctypes.c_float),
+                ("seed", ctypes.c_uint32), ("reserved", ctypes.c_uint32 * 4)]
+
+
+class MlpTrainReport(ctypes.Structure):
+    _fields_ = [("samples", ctypes.c_uint64), ("positives", ctypes.c_uint64), ("puzzles", ctypes.c_uint32),
+                ("epochs", ctypes.c_uint32), ("first_loss", ctypes.c_double), ("last_loss", ctypes.c_double),
+                ("train_ms", ctypes.c_double)]
+
+
+MLP_INPUTS = 512
+MLP_HIDDEN = 256
+MLP_PARAMS = 256 * 512 + 256 + 256 * 256 + 256 + 256 + 1
+
+
 class GmConfig(ctypes.Structure):
     _fields_ = [("push_budget", ctypes.c_uint64), ("timeout_ms", ctypes.c_uint32), ("device", ctypes.c_int32),
                 ("placement_budget", ctypes.c_uint64), ("reserved", ctypes.c_uint32 * 6)]
@@ -137,6 +153,19 @@ SIGNATURES = {
     "emp_bt_plan_destroy": (None, [ctypes.c_void_p]),
     "emp_bt_autotune": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_uint32, ctypes.POINTER(BtConfig), ctypes.c_uint32,
                                          ctypes.POINTER(TuneResult)]),
+    "emp_mlp_create": (ctypes.c_int32, [ctypes.c_uint64, ctypes.c_int32, ctypes.POINTER(ctypes.c_void_p)]),
+    "emp_mlp_destroy": (None, [ctypes.c_void_p]),
+    "emp_mlp_get_params": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_void_p]),
+    "emp_mlp_set_params": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_void_p]),
+    "emp_mlp_features": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p,
+                                          ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p]),
+    "emp_mlp_score": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p]),
+    "emp_mlp_score_f32": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p]),
+    "emp_mlp_loss_grad": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                           ctypes.c_uint64, ctypes.POINTER(ctypes.c_double), ctypes.c_void_p]),
+    "emp_mlp_train": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p,
+                                       ctypes.POINTER(MlpTrainConfig), ctypes.POINTER(MlpTrainReport)]),
+    "emp_bt_plan_order": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_void_p]),
     "emp_glutton_max": (ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(GmConfig), ctypes.POINTER(GmResult)]),
     "emp_glutton_max_noalloc": (ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(GmConfig), ctypes.POINTER(GmResult)]),
 }
@@ -248,6 +277,102 @@ def bt_autotune(puzzles: Sequence[NativePuzzle], trial_ms: int = 200, **kw) -> T
     return out
 
 
+def _f32(a, n=None):
+    import numpy as np
+    arr = np.ascontiguousarray(a, dtype=np.float32)
+    if n is not None and arr.size != n:
+        raise ValueError(f"expected {n} values, got {arr.size}")
+    return arr
+
+
+class Mlp:
+    """emp_mlp: the candidate-scoring network of the learned value ordering."""
+
+    def __init__(self, seed: int = 1, device: int = -1):
+        h = ctypes.c_void_p()
+        check(load().emp_mlp_create(seed, device, ctypes.byref(h)))
+        self.handle = h.value
+
+    def close(self) -> None:
+        if self.handle:
+            load().emp_mlp_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def params(self):
+        import numpy as np
+        out = np.empty(MLP_PARAMS, dtype=np.float32)
+        check(load().emp_mlp_get_params(self.handle, out.ctypes.data))
+        return out
+
+    def set_params(self, params) -> None:
+        arr = _f32(params, MLP_PARAMS)
+        check(load().emp_mlp_set_params(self.handle, arr.ctypes.data))
+
+    def score(self, features):
+        """Tensor-core scores (BF16 operands, FP32 accumulation)."""
+        import numpy as np
+        x = _f32(features)
+        n = x.size // MLP_INPUTS
+        out = np.empty(n, dtype=np.float32)
+        check(load().emp_mlp_score(self.handle, x.ctypes.data, n, out.ctypes.data))
+        return out
+
+    def score_f32(self, features):
+        import numpy as np
+        x = _f32(features)
+        n = x.size // MLP_INPUTS
+        out = np.empty(n, dtype=np.float32)
+        check(load().emp_mlp_score_f32(self.handle, x.ctypes.data, n, out.ctypes.data))
+        return out
+
+    def loss_grad(self, features, labels, weights):
+        import numpy as np
+        x = _f32(features)
+        n = x.size // MLP_INPUTS
+        y = _f32(labels, n)
+        w = _f32(weights, n)
+        loss = ctypes.c_double()
+        grads = np.empty(MLP_PARAMS, dtype=np.float32)
+        check(load().emp_mlp_loss_grad(self.handle, x.ctypes.data, y.ctypes.data, w.ctypes.data, n,
+                                       ctypes.byref(loss), grads.ctypes.data))
+        return loss.value, grads
+
+    def train(self, puzzles: Sequence[NativePuzzle], solutions, epochs: int = 0, batch: int = 0,
+              learning_rate: float = 0.0, seed: int = 1) -> MlpTrainReport:
+        """solutions: one emp_bt_result.first_solution board (256 values) per puzzle."""
+        import numpy as np
+        arr = (ctypes.c_void_p * len(puzzles))(*[p.handle for p in puzzles])
+        boards = np.ascontiguousarray(solutions, dtype=np.uint32).reshape(len(puzzles), 256)
+        cfg = MlpTrainConfig()
+        cfg.epochs, cfg.batch, cfg.learning_rate, cfg.seed = epochs, batch, learning_rate, seed
+        rep = MlpTrainReport()
+        check(load().emp_mlp_train(self.handle, arr, len(puzzles), boards.ctypes.data, ctypes.byref(cfg),
+                                   ctypes.byref(rep)))
+        return rep
+
+
+def mlp_features(puzzle: NativePuzzle, prefixes: Sequence[Sequence[int]], cands: Sequence[int]):
+    """emp_mlp_features: one row per (prefix, candidate placed right after it)."""
+    import numpy as np
+    n = len(prefixes)
+    stride = max([len(p) for p in prefixes] + [1])
+    pre = np.zeros((n, stride), dtype=np.uint16)
+    for i, p in enumerate(prefixes):
+        pre[i, :len(p)] = p
+    lens = np.array([len(p) for p in prefixes], dtype=np.uint16)
+    cd = np.array(cands, dtype=np.uint16)
+    out = np.empty((n, MLP_INPUTS), dtype=np.float32)
+    check(load().emp_mlp_features(puzzle.handle, pre.ctypes.data, stride, lens.ctypes.data, cd.ctypes.data, n,
+                                  out.ctypes.data))
+    return out
+
+
 def config_dict(cfg: BtConfig) -> dict:
     return {name: getattr(cfg, name) for name, _ in BtConfig._fields_}
 
@@ -304,6 +429,10 @@ class BtPlan:
         res = (BtResult * len(self.puzzles))()
         check(load().emp_bt_plan_results(self.handle, res))
         return list(res)
+
+    def order(self, model: "Mlp") -> None:
+        """emp_bt_plan_order: queue the subtrees best first by the model's scores."""
+        check(load().emp_bt_plan_order(self.handle, model.handle))
 
     def subtree_counts(self, count: int):
         nn = (ctypes.c_uint64 * count)()

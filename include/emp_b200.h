@@ -200,6 +200,79 @@ typedef struct emp_bt_tune_result {
 emp_status emp_bt_autotune(const emp_puzzle *puzzles, uint32_t count, const emp_bt_config *base,
                            uint32_t trial_ms, emp_bt_tune_result *out);
 
+/* ---------------- learned value ordering (no counterpart in the reference) ----------------
+ *
+ * A network scores candidate placements (position, piece, rotation) from 512
+ * features of the placement and the pieces already placed: one-hot side colours,
+ * neighbour states, how many edges of each free side's colour remain on unplaced
+ * pieces, position, depth and kind.  It has two hidden layers of 256 (relu) and one
+ * output s; sigmoid(s) reads as the chance that the placement lies on a solution
+ * path.  Inference runs on the tensor cores (BF16 operands, FP32 accumulation),
+ * training in f32 CUDA kernels.  Ordering changes only which subtrees are searched
+ * first: the set of subtrees and the search below them are those of the plain
+ * order, so exhaustive counts do not change. */
+
+#define EMP_MLP_INPUTS 512u
+#define EMP_MLP_HIDDEN 256u
+/* parameters in this order: W1[256][512], b1[256], W2[256][256], b2[256], w3[256], b3 */
+#define EMP_MLP_PARAMS (256u * 512u + 256u + 256u * 256u + 256u + 256u + 1u)
+
+typedef struct emp_mlp_t *emp_mlp;
+
+/* A network with seeded random weights (uniform, scaled by 1/sqrt(fan-in)) on a device. */
+emp_status emp_mlp_create(uint64_t seed, int32_t device, emp_mlp *out);
+void emp_mlp_destroy(emp_mlp model);
+emp_status emp_mlp_get_params(emp_mlp model, float *params);        /* EMP_MLP_PARAMS values */
+emp_status emp_mlp_set_params(emp_mlp model, const float *params);
+
+/* Feature rows of n candidates: candidate cands[i] placed at level lens[i] after the
+ * transitions prefixes[i*stride .. i*stride+lens[i]) of the puzzle's order.  out
+ * receives n * EMP_MLP_INPUTS values (0 or 1). */
+emp_status emp_mlp_features(emp_puzzle puzzle, const uint16_t *prefixes, uint32_t stride, const uint16_t *lens,
+                            const uint16_t *cands, uint64_t n, float *out);
+
+/* Scores of n feature rows on the tensor cores (features rounded to BF16). */
+emp_status emp_mlp_score(emp_mlp model, const float *features, uint64_t n, float *scores);
+/* Same network in f32 on the CUDA cores (the training forward pass). */
+emp_status emp_mlp_score_f32(emp_mlp model, const float *features, uint64_t n, float *scores);
+
+/* Weighted logistic loss of n rows with labels in {0,1}: loss = sum w (softplus(s) - y s) / sum w,
+ * and its gradient with respect to every parameter (EMP_MLP_PARAMS values). */
+emp_status emp_mlp_loss_grad(emp_mlp model, const float *features, const float *labels, const float *weights,
+                             uint64_t n, double *loss, float *grads);
+
+typedef struct emp_mlp_train_config {
+    uint32_t epochs;             /* passes over the samples; 0 = 30 */
+    uint32_t batch;              /* rows per step; 0 = 2048 */
+    float learning_rate;         /* Adam step size; 0 = 1e-3 */
+    uint32_t seed;               /* shuffling */
+    uint32_t reserved[4];
+} emp_mlp_train_config;
+
+typedef struct emp_mlp_train_report {
+    uint64_t samples;            /* candidate placements seen by training */
+    uint64_t positives;          /* of them on the solution paths */
+    uint32_t puzzles;            /* puzzles with a solution path */
+    uint32_t epochs;
+    double first_loss;           /* mean weighted loss of the first and the last epoch */
+    double last_loss;
+    double train_ms;
+} emp_mlp_train_report;
+
+/* Trains the network on the solver's traces: for every puzzle with a solution
+ * (solutions[i*256 ..] in the emp_bt_result.first_solution format, 0xFFFFFFFF for
+ * none), every level of the solution path gives one positive (the solution's
+ * placement) and its siblings (the other candidates the search tries at that node)
+ * as negatives; positives are weighted to balance the two classes. */
+emp_status emp_mlp_train(emp_mlp model, const emp_puzzle *puzzles, uint32_t count, const uint32_t *solutions,
+                         const emp_mlp_train_config *config, emp_mlp_train_report *report);
+
+/* Queues the plan's subtrees best first: every prefix gets the sum over its levels of
+ * log sigmoid(score of the placement), and within each puzzle the subtrees run in
+ * decreasing order of that sum.  Counts stay those of the plain order; stop_at_first
+ * (the lexicographically first solution) is not available on an ordered plan. */
+emp_status emp_bt_plan_order(emp_bt_plan plan, emp_mlp model);
+
 /* ---------------- glutton max search (CUDA_glutton_max semantics) ---------------- */
 
 typedef struct emp_gm_config {
