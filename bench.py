@@ -394,6 +394,85 @@ def run_glutton(args, rank, world, local_rank):
     print(json.dumps(out), flush=True)
 
 
+LEARN_TRAIN_SEEDS = range(1000, 1064)
+LEARN_EVAL_SEEDS = range(100, 164)
+LEARN_TIMEOUT_MS = 30000
+LEARN_WORKLOAD = ("time to a first solution of 64 seeded 8x8 puzzles (4 border / 8 interior colours, seeds "
+                  "100..163), split depth 12, stop at the first solution any thread finds; plain order against "
+                  "subtrees queued best first by the network trained on the solver's solution paths of seeds "
+                  "1000..1063 (the ordering's scoring and sort are counted in its time)")
+
+
+def run_learned(args, rank, world, local_rank):
+    """Learned value ordering: median time and placements to a first solution, plain vs learned."""
+    import torch
+    from edge_matching_puzzle_b200 import native
+    from edge_matching_puzzle_b200.puzzle import generate
+    torch.cuda.set_device(local_rank)
+    if rank != 0:
+        return
+    t_train0 = time.perf_counter()
+    train_h, boards = [], []
+    for s in LEARN_TRAIN_SEEDS:
+        pz = generate(WIDTH, HEIGHT, BORDER, INTERIOR, s)
+        h = native.NativePuzzle(WIDTH, HEIGHT, pz.colors)
+        r = native.bt_count(h, split_depth=DEPTH, stop_at_any=1, timeout_ms=LEARN_TIMEOUT_MS, device=local_rank)
+        if r.has_first_solution:
+            train_h.append(h)
+            boards.append(list(r.first_solution))
+    model = native.Mlp(seed=1, device=local_rank)
+    rep = model.train(train_h, boards, epochs=args.learn_epochs, batch=2048, learning_rate=1e-3)
+    train_s = time.perf_counter() - t_train0
+    rows = []
+    for s in LEARN_EVAL_SEEDS:
+        pz = generate(WIDTH, HEIGHT, BORDER, INTERIOR, s)
+        h = native.NativePuzzle(WIDTH, HEIGHT, pz.colors)
+        out = {"seed": s}
+        for arm in ("plain", "learned"):
+            plan = native.BtPlan([h], split_depth=DEPTH, stop_at_any=1, timeout_ms=LEARN_TIMEOUT_MS, device=local_rank)
+            order_ms = 0.0
+            if arm == "learned":
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                plan.order(model)
+                torch.cuda.synchronize()
+                order_ms = 1000 * (time.perf_counter() - t0)
+            plan.run()
+            r = plan.results()[0]
+            found = r.first_found_us > 0
+            ms = (r.first_found_us / 1000.0 if found else r.kernel_ms) + order_ms
+            out[arm] = {"found": found, "ms": ms, "nodes": r.nodes, "order_ms": order_ms,
+                        "complete": r.status == native.EMP_OK}
+            plan.close()
+        rows.append(out)
+    solved = [r for r in rows if r["plain"]["found"] and r["learned"]["found"]]
+    med = lambda xs: statistics.median(xs) if xs else None  # noqa: E731
+    plain_ms = med([r["plain"]["ms"] for r in solved])
+    learned_ms = med([r["learned"]["ms"] for r in solved])
+    if args.counts_out:
+        with open(args.counts_out, "w") as f:
+            for r in rows:
+                f.write(json.dumps(r) + "\n")
+    out = {
+        "metric": METRIC, "value": learned_ms, "unit": "ms to a first solution (median)", "n_gpus": 1,
+        "steps": len(rows), "warmup": 0, "ms_per_step": learned_ms, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u64 search, bf16 network", "data": "synthetic",
+        "config": {"workload": LEARN_WORKLOAD, "puzzles_with_solution": len(solved), "puzzles": len(rows),
+                   "train": {"puzzles": rep.puzzles, "samples": rep.samples, "positives": rep.positives,
+                             "epochs": rep.epochs, "first_loss": rep.first_loss, "last_loss": rep.last_loss,
+                             "seconds_incl_traces": train_s}},
+        "plain_median_ms": plain_ms,
+        "learned_median_ms": learned_ms,
+        "speedup_median_time": plain_ms / learned_ms if plain_ms and learned_ms else None,
+        "plain_median_nodes": med([r["plain"]["nodes"] for r in solved]),
+        "learned_median_nodes": med([r["learned"]["nodes"] for r in solved]),
+        "median_order_ms": med([r["learned"]["order_ms"] for r in solved]),
+        "gpu_launches": None,
+        "e2e": None,
+    }
+    print(json.dumps(out), flush=True)
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -429,9 +508,11 @@ def main():
     ap.add_argument("--full", action="store_true", help="run all slices (the complete count) and print per-seed totals")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
-    ap.add_argument("--workload", default="exhaustive", choices=["exhaustive", "batch", "glutton"],
+    ap.add_argument("--workload", default="exhaustive", choices=["exhaustive", "batch", "glutton", "learned"],
                     help="exhaustive: the 16 seeded 8x8 puzzles (default); batch: 4096 mixed instances; "
-                         "glutton: the 16x16 glutton max search")
+                         "glutton: the 16x16 glutton max search; learned: time to a first solution, plain vs "
+                         "learned value ordering")
+    ap.add_argument("--learn-epochs", type=int, default=20, help="learned: training epochs")
     ap.add_argument("--gm-budget", type=int, default=0,
                     help="glutton: placement budget of each search (0: a time-bounded step)")
     ap.add_argument("--counts-out", default=None, help="batch: write per-instance counts (JSON lines) here")
@@ -454,6 +535,9 @@ def main():
         return
     if args.workload == "glutton":
         run_glutton(args, rank, world, local_rank)
+        return
+    if args.workload == "learned":
+        run_learned(args, rank, world, local_rank)
         return
 
     import torch
