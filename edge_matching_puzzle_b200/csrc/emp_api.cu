@@ -166,6 +166,20 @@ emp_status expand(emp_bt_plan_t& pl)
                                            child_puzzle.as<uint32_t>(), lnodes, lnodes + P, 1, fz, st));
         std::swap(parents, children);
         std::swap(parent_puzzle, child_puzzle);
+        if (pl.dump) {
+            // keep this level's prefixes (length level + 1) for the solution indices
+            if (pl.level_prefixes.size() < level + 2) {
+                pl.level_prefixes.resize(level + 2);
+                pl.level_counts.resize(level + 2, 0);
+            }
+            DeviceBuffer keep;
+            CUDA_TRY(keep.alloc(sizeof(uint16_t) * std::max<uint64_t>(total, 1) * (level + 1)));
+            if (total)
+                CUDA_TRY(cudaMemcpyAsync(keep.p, parents.p, sizeof(uint16_t) * total * (level + 1),
+                                         cudaMemcpyDeviceToDevice, st));
+            pl.level_prefixes[level + 1] = std::move(keep);
+            pl.level_counts[level + 1] = total;
+        }
         np = total;
         if (pl.adaptive) {
             // placements of this level per puzzle = its prefixes after this level
@@ -227,8 +241,21 @@ emp_status plan_build_initial(emp_bt_plan_t& pl, uint64_t first, uint64_t stride
     return EMP_OK;
 }
 
+namespace {
+emp_status create_plan(const emp_puzzle* puzzles, uint32_t count, const emp_bt_config* config, bool dump,
+                       emp_bt_plan* out);
+}  // namespace
+
 extern "C" emp_status emp_bt_plan_create(const emp_puzzle* puzzles, uint32_t count, const emp_bt_config* config,
                                          emp_bt_plan* out)
+{
+    return create_plan(puzzles, count, config, false, out);
+}
+
+namespace {
+
+emp_status create_plan(const emp_puzzle* puzzles, uint32_t count, const emp_bt_config* config, bool dump,
+                       emp_bt_plan* out)
 {
     emp::clear_error();
     if (!puzzles || !count || !out) return fail(EMP_ERR_INVALID, "emp_bt_plan_create: no puzzle");
@@ -282,6 +309,7 @@ extern "C" emp_status emp_bt_plan_create(const emp_puzzle* puzzles, uint32_t cou
     CUDA_TRY(cudaEventCreate(&pl->evr0));
     CUDA_TRY(cudaEventCreate(&pl->evr1));
     if (pl->cfg.use_graph) CUDA_TRY(cudaStreamCreateWithFlags(&pl->capture_stream, cudaStreamNonBlocking));
+    pl->dump = dump;
     EMP_TRY(expand(*pl));
     // hot tables in shared memory when the plan holds one puzzle
     const uint32_t hot = (pl->puzzles[0]->tables.blob[26] + 3u) & ~3u;
@@ -328,6 +356,8 @@ extern "C" emp_status emp_bt_plan_create(const emp_puzzle* puzzles, uint32_t cou
     *out = pl.release();
     return EMP_OK;
 }
+
+}  // namespace
 
 extern "C" emp_status emp_bt_plan_subtrees(emp_bt_plan plan, uint64_t* subtrees)
 {
@@ -631,4 +661,80 @@ extern "C" emp_status emp_bt_count_batch(const emp_puzzle* puzzles, uint32_t cou
 extern "C" emp_status emp_bt_count(emp_puzzle puzzle, const emp_bt_config* config, emp_bt_result* result)
 {
     return emp_bt_count_batch(&puzzle, 1, config, result);
+}
+
+extern "C" emp_status emp_bt_solutions(emp_puzzle puzzle, const emp_bt_config* config, emp_bt_solution* out,
+                                       uint64_t capacity, uint64_t* found, emp_bt_result* result)
+{
+    emp::clear_error();
+    if (!puzzle || !found || (capacity && !out)) return fail(EMP_ERR_INVALID, "emp_bt_solutions: null argument");
+    emp_bt_config cfg{};
+    cfg.device = -1;
+    if (config) cfg = *config;
+    cfg.keep_subtree_counts = 1;
+    cfg.stop_at_first = 0;
+    cfg.stop_at_any = 0;
+    cfg.sample_stride = 0;
+    cfg.use_graph = 0;
+    cfg.split_subtrees = 0;
+    emp_bt_plan plan = nullptr;
+    emp_status s = create_plan(&puzzle, 1, &cfg, true, &plan);
+    if (s != EMP_OK) return s;
+    std::unique_ptr<emp_bt_plan_t> guard(plan);
+    plan->budget = 0;  // never hand work back: each subtree is searched in order by one thread
+    const uint64_t cap = std::max<uint64_t>(capacity, 1);
+    CUDA_TRY(plan->sol_buf.alloc(sizeof(emp::SolutionRecord) * cap));
+    CUDA_TRY(plan->sol_count.alloc(sizeof(unsigned long long)));
+    CUDA_TRY(cudaMemset(plan->sol_count.p, 0, sizeof(unsigned long long)));
+    plan->sol_capacity = capacity;
+    s = emp_bt_plan_run(plan, nullptr);
+    if (s != EMP_OK) return s;
+    emp_bt_result res{};
+    s = emp_bt_plan_results(plan, &res);
+    if (s != EMP_OK) return s;
+    if (result) *result = res;
+    if (res.status != EMP_OK) return fail(EMP_INCOMPLETE, "emp_bt_solutions: the search stopped before the end");
+    unsigned long long total = 0;
+    CUDA_TRY(cudaMemcpy(&total, plan->sol_count.p, sizeof(total), cudaMemcpyDeviceToHost));
+    *found = total;
+    const uint64_t nsol = std::min<uint64_t>(total, capacity);
+    if (!nsol) return EMP_OK;
+    // level arrays: device pointer table (index L = prefixes of length L)
+    const uint32_t depth = plan->depth;
+    std::vector<const uint16_t*> ptrs(depth + 1, nullptr);
+    std::vector<uint64_t> counts(depth + 1, 0);
+    for (uint32_t L = 1; L <= depth && L < plan->level_prefixes.size(); ++L) {
+        ptrs[L] = plan->level_prefixes[L].as<uint16_t>();
+        counts[L] = plan->level_counts[L];
+    }
+    DeviceBuffer d_ptrs, d_counts, d_idx;
+    CUDA_TRY(d_ptrs.alloc(sizeof(void*) * ptrs.size()));
+    CUDA_TRY(d_counts.alloc(sizeof(uint64_t) * counts.size()));
+    CUDA_TRY(d_idx.alloc(sizeof(unsigned long long) * nsol));
+    CUDA_TRY(cudaMemcpy(d_ptrs.p, ptrs.data(), sizeof(void*) * ptrs.size(), cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(d_counts.p, counts.data(), sizeof(uint64_t) * counts.size(), cudaMemcpyHostToDevice));
+    CUDA_TRY(emp::launch_solution_index(plan->sol_buf.as<emp::SolutionRecord>(), nsol,
+                                        reinterpret_cast<const uint16_t* const*>(d_ptrs.p), d_counts.as<uint64_t>(),
+                                        depth, plan->item_nodes.as<unsigned long long>(),
+                                        d_idx.as<unsigned long long>(), nullptr));
+    std::vector<emp::SolutionRecord> recs(nsol);
+    std::vector<unsigned long long> idx(nsol);
+    CUDA_TRY(cudaMemcpy(recs.data(), plan->sol_buf.p, sizeof(emp::SolutionRecord) * nsol, cudaMemcpyDeviceToHost));
+    CUDA_TRY(cudaMemcpy(idx.data(), d_idx.p, sizeof(unsigned long long) * nsol, cudaMemcpyDeviceToHost));
+    std::vector<uint64_t> order(nsol);
+    for (uint64_t i = 0; i < nsol; ++i) order[i] = i;
+    std::sort(order.begin(), order.end(), [&](uint64_t a, uint64_t b) { return idx[a] < idx[b]; });
+    const emp::PuzzleModel& m = puzzle->model;
+    for (uint64_t k = 0; k < nsol; ++k) {
+        const emp::SolutionRecord& r = recs[order[k]];
+        emp_bt_solution& o = out[k];
+        o.node_index = idx[order[k]];
+        for (uint32_t pos = 0; pos < 256; ++pos) o.board[pos] = 0xFFFFFFFFu;
+        for (uint32_t l = 0; l < m.n; ++l) {
+            const emp::LevelPlan& lp = puzzle->plan[l];
+            const uint32_t t = r.t[l];
+            o.board[lp.position] = (m.members[lp.kind][t >> 2] << 2) | (t & 3u);
+        }
+    }
+    return EMP_OK;
 }

@@ -651,6 +651,16 @@ __global__ void __launch_bounds__(T) dfs_kernel(BtLaunch P)
                 if (dfs_step<KW, SM, T>(P, s, stk, av, spill, &solved)) {
                     if (solved) {
                         record_solution<T>(P, s, stk);
+                        if (P.sols) {
+                            const unsigned long long slot = atomicAdd(P.sol_count, 1ull);
+                            if (slot < P.sol_capacity) {
+                                SolutionRecord* r = P.sols + slot;
+                                r->orig = s.orig;
+                                r->local = s.nodes;
+                                for (uint32_t l = 0; l < s.n; ++l)
+                                    r->t[l] = static_cast<uint16_t>((stk[l * T] >> 21) & 0x3FFu);
+                            }
+                        }
                         if (P.stop_at_any) {
                             // first solution of the run: note the time and stop every thread
                             atomicCAS(&P.ctl->first_found_ns, 0ull, static_cast<unsigned long long>(global_ns()));
@@ -777,6 +787,45 @@ __global__ void round_copy_kernel(BtLaunch P, uint4* __restrict__ dst, const uin
     const uint64_t tail = vec * 4 + blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
     if (tail < words)
         reinterpret_cast<uint32_t*>(dst)[tail] = reinterpret_cast<const uint32_t*>(src)[tail];
+}
+
+// One block per solution: thread 0 binary-searches the level arrays, the block
+// sums the counts of the subtrees before the solution's own.
+__global__ void solution_index_kernel(const SolutionRecord* __restrict__ sols, const uint16_t* const* level_prefixes,
+                                      const uint64_t* __restrict__ level_counts, uint32_t depth,
+                                      const unsigned long long* __restrict__ item_nodes, unsigned long long* out)
+{
+    __shared__ unsigned long long part[256];
+    const SolutionRecord& s = sols[blockIdx.x];
+    unsigned long long acc = 0;
+    for (unsigned long long j = threadIdx.x; j < s.orig; j += blockDim.x) acc += item_nodes[j];
+    part[threadIdx.x] = acc;
+    __syncthreads();
+    for (uint32_t w = blockDim.x / 2; w; w >>= 1) {
+        if (threadIdx.x < w) part[threadIdx.x] += part[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        unsigned long long exp_before = 0;
+        for (uint32_t L = 1; L <= depth; ++L) {
+            // level arrays hold the prefixes of length L in lexicographic order:
+            // count those at or before the solution's first L transitions
+            const uint16_t* a = level_prefixes[L];
+            uint64_t lo = 0, hi = level_counts[L];
+            while (lo < hi) {
+                const uint64_t mid = (lo + hi) / 2;
+                int cmp = 0;
+                for (uint32_t l = 0; l < L && !cmp; ++l) {
+                    const uint16_t x = a[mid * L + l];
+                    cmp = x < s.t[l] ? -1 : (x > s.t[l] ? 1 : 0);
+                }
+                if (cmp <= 0) lo = mid + 1;
+                else hi = mid;
+            }
+            exp_before += lo;
+        }
+        out[blockIdx.x] = exp_before + part[0] + s.local;
+    }
 }
 
 // Prefix (transitions) of selected subtree `i`, for the host.
@@ -918,6 +967,16 @@ cudaError_t launch_make_records(const uint16_t* prefixes, const uint32_t* prefix
     const uint64_t blocks = std::min<uint64_t>((count + 255) / 256, 148ull * 32);
     make_records<<<(unsigned)blocks, 256, 0, stream>>>(prefixes, prefix_puzzle, depth, first, stride, count,
                                                        rec_words, rec, puzzle_depth);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_solution_index(const SolutionRecord* sols, uint64_t nsol, const uint16_t* const* level_prefixes,
+                                  const uint64_t* level_counts, uint32_t depth, const unsigned long long* item_nodes,
+                                  unsigned long long* out, cudaStream_t stream)
+{
+    if (!nsol) return cudaSuccess;
+    solution_index_kernel<<<static_cast<unsigned>(nsol), 256, 0, stream>>>(sols, level_prefixes, level_counts, depth,
+                                                                           item_nodes, out);
     return cudaGetLastError();
 }
 

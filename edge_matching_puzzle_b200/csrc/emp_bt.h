@@ -24,6 +24,15 @@ struct FirstRecord {
     uint16_t t[256];        // transition per level
 };
 
+// One solution found by a thread (solution dumps): its subtree, the placements of the
+// subtree searched up to and including it (one thread searches the whole subtree in
+// order), and its path.
+struct SolutionRecord {
+    unsigned long long orig;
+    unsigned long long local;
+    uint16_t t[256];
+};
+
 // Run state on the device, shared by the launches of one run.
 struct BtRunCtl {
     unsigned long long deadline;     // absolute %globaltimer deadline of the run; 0 = none
@@ -67,6 +76,9 @@ struct BtLaunch {
     BtRunCtl* ctl = nullptr;                  // deadline; in graph runs also the round's record count
     int n_in_from_ctl = 0;                    // 1: read the round's record count from ctl->n_in
     uint32_t* incomplete = nullptr;           // per puzzle: 1 when some of its work was dropped (deadline, abort)
+    SolutionRecord* sols = nullptr;           // solution dumps: every solution found (null: not recorded)
+    unsigned long long* sol_count = nullptr;
+    unsigned long long sol_capacity = 0;
 };
 
 cudaError_t launch_expand(const BtLaunch& P, const uint16_t* parents, const uint32_t* parent_puzzle,
@@ -98,6 +110,12 @@ cudaError_t launch_make_records(const uint16_t* prefixes, const uint32_t* prefix
 cudaError_t launch_round_advance(const BtLaunch& P, cudaGraphConditionalHandle loop, uint32_t max_rounds,
                                  cudaStream_t stream);
 cudaError_t launch_round_copy(const BtLaunch& P, uint32_t* dst, const uint32_t* src, cudaStream_t stream);
+// Solution dumps: for solution j, out[j] = placements of the sequential search up to
+// and including it = (expansion nodes lexicographically at or before its prefix, one
+// binary search per level array) + (counts of the subtrees before its own) + its local count.
+cudaError_t launch_solution_index(const SolutionRecord* sols, uint64_t nsol, const uint16_t* const* level_prefixes,
+                                  const uint64_t* level_counts, uint32_t depth, const unsigned long long* item_nodes,
+                                  unsigned long long* out, cudaStream_t stream);
 cudaError_t launch_record_prefix(const uint32_t* rec, uint32_t rec_words, uint64_t i, uint16_t* out,
                                  cudaStream_t stream);
 const void* dfs_kernel_symbol(uint32_t max_kw, bool smem_tables, uint32_t threads);

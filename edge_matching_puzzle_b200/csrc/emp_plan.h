@@ -31,6 +31,13 @@ struct emp_bt_plan_t {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
     bool graph_ran = false;
+    // solution dumps: the expansion's level arrays (prefixes of length L at [L]) and
+    // the solutions found
+    bool dump = false;
+    std::vector<DeviceBuffer> level_prefixes;
+    std::vector<uint64_t> level_counts;
+    DeviceBuffer sol_buf, sol_count;
+    uint64_t sol_capacity = 0;
     uint64_t n_all = 0, n_init = 0;
     bool sampled = false;
     std::vector<unsigned long long> exp_nodes, exp_sols;
@@ -87,6 +94,9 @@ struct emp_bt_plan_t {
         P.stop_at_first = cfg.stop_at_first ? 1 : 0;
         P.stop_at_any = cfg.stop_at_any ? 1 : 0;
         P.ctl = ctl.as<emp::BtRunCtl>();
+        P.sols = sol_buf.as<emp::SolutionRecord>();
+        P.sol_count = sol_count.as<unsigned long long>();
+        P.sol_capacity = sol_capacity;
         P.incomplete = incomplete.as<uint32_t>();
         return P;
     }

@@ -1,6 +1,7 @@
 // C++ host layer over the C ABI: features, factory, parser, strategy generators.
 #include "emp_host.h"
 
+#include <algorithm>
 #include <chrono>
 #include <fstream>
 #include <sstream>
@@ -159,6 +160,74 @@ void feature_CUDA_backtracker::run()
     m_out << "Total elapsed time: " << elapsed.count() << "s" << std::endl;
 }
 
+void write_results_bin(const std::string& path, const emp_piece_set& pieces, const emp_strategy_generator& strategy,
+                       const std::vector<emp_bt_solution>& solutions, uint64_t total_nodes)
+{
+    std::ofstream f(path, std::ios::binary);
+    if (!f) throw emp_logic_error("Unable to open file \"" + path + "\" for writing", __LINE__, __FILE__);
+    const uint32_t n = pieces.size();
+    auto put32 = [&](uint32_t v) { f.write(reinterpret_cast<const char*>(&v), 4); };
+    auto put64 = [&](uint64_t v) { f.write(reinterpret_cast<const char*>(&v), 8); };
+    put32(1);
+    put32(pieces.width);
+    put32(pieces.height);
+    put32(1);
+    for (uint32_t i = 0; i < n; ++i) {
+        const auto xy = strategy.get_position(i);
+        put32(xy.first);
+        put32(xy.second);
+    }
+    uint32_t id_bits = 0;
+    for (uint32_t v = n - 1; v; v >>= 1) ++id_bits;
+    const uint32_t field = id_bits + 2;
+    std::vector<uint64_t> words((static_cast<uint64_t>(n) * field + 63) / 64);
+    for (const emp_bt_solution& s : solutions) {
+        std::fill(words.begin(), words.end(), 0);
+        for (uint32_t i = 0; i < n; ++i) {
+            const uint32_t v = s.board[strategy.order()[i]];
+            for (uint32_t b = 0; b < field; ++b)
+                if ((v >> b) & 1u) {
+                    const uint64_t bit = static_cast<uint64_t>(i) * field + b;
+                    words[bit >> 6] |= 1ull << (bit & 63);
+                }
+        }
+        f.write(reinterpret_cast<const char*>(words.data()), static_cast<std::streamsize>(8 * words.size()));
+        put64(s.node_index);
+    }
+    put64(total_nodes);
+    if (!f) throw emp_logic_error("Write error on \"" + path + "\"", __LINE__, __FILE__);
+}
+
+feature_new_strategy::feature_new_strategy(const emp_piece_set& pieces, const emp_strategy_generator& strategy,
+                                           const std::string& dump_file, const feature_options& options,
+                                           std::ostream& out)
+    : m_pieces(pieces), m_strategy(strategy), m_dump_file(dump_file), m_options(options), m_out(out)
+{
+}
+
+void feature_new_strategy::run()
+{
+    emp_puzzle_owner puzzle(m_pieces, &m_strategy);
+    emp_bt_config cfg{};
+    cfg.device = m_options.device;
+    cfg.split_depth = m_options.split_depth;
+    cfg.timeout_ms = m_options.timeout_ms;
+    std::vector<emp_bt_solution> sols(1024);
+    uint64_t found = 0;
+    emp_bt_result res{};
+    emp_status st = emp_bt_solutions(puzzle.get(), &cfg, sols.data(), sols.size(), &found, &res);
+    if (st == EMP_OK && found > sols.size()) {
+        sols.resize(found);
+        st = emp_bt_solutions(puzzle.get(), &cfg, sols.data(), sols.size(), &found, &res);
+    }
+    if (st != EMP_OK) throw_abi("emp_bt_solutions", st, __LINE__);
+    sols.resize(found);
+    write_results_bin(m_dump_file, m_pieces, m_strategy, sols, res.nodes);
+    m_out << "End of algorithm" << std::endl;
+    m_out << "Total situations explored : " << res.nodes << std::endl;
+    m_out << "Nb solutions : " << res.solutions << std::endl;
+}
+
 feature_CUDA_glutton_max::feature_CUDA_glutton_max(const emp_piece_set& pieces, const feature_options& options,
                                                    std::ostream& out)
     : m_pieces(pieces), m_options(options), m_out(out)
@@ -186,8 +255,14 @@ void feature_CUDA_glutton_max::run()
 
 feature_if& factory_feature::create_feature(const std::string& feature_name, const emp_piece_set& pieces,
                                             std::unique_ptr<emp_strategy_generator>& strategy,
-                                            const feature_options& options, std::ostream& out)
+                                            const feature_options& options, std::ostream& out,
+                                            const std::string& dump_file)
 {
+    if (feature_name == "new_strategy") {
+        // the reference's default order for this feature is the spiral (src/main.cpp:103-106)
+        if (!strategy) strategy = create_strategy_generator("spiral", pieces.width, pieces.height);
+        return *new feature_new_strategy(pieces, *strategy, dump_file, options, out);
+    }
     if (feature_name == "CUDA_backtracker") {
         if (!strategy) strategy = create_strategy_generator("basic", pieces.width, pieces.height);
         return *new feature_CUDA_backtracker(pieces, *strategy, options, out);

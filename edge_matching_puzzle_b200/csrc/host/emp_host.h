@@ -134,6 +134,30 @@ class feature_CUDA_backtracker : public feature_if {
     emp_bt_result m_result{};
 };
 
+// The reference's solution file (include/emp_situation_binary_dumper.h:58-124):
+// header, visiting order, one record per solution (the placed pieces of each level
+// packed on bits(n-1)+2 bits, then the node index) and the final node count.
+void write_results_bin(const std::string& path, const emp_piece_set& pieces, const emp_strategy_generator& strategy,
+                       const std::vector<emp_bt_solution>& solutions, uint64_t total_nodes);
+
+// The exhaustive search of emp_strategy (feature new_strategy) run on the GPU: every
+// solution in the reference's order, written to the dump file, and the totals.  The
+// reference's "New max" progress lines belong to its sequential walk and are not printed.
+class feature_new_strategy : public feature_if {
+  public:
+    feature_new_strategy(const emp_piece_set& pieces, const emp_strategy_generator& strategy,
+                         const std::string& dump_file, const feature_options& options = {},
+                         std::ostream& out = std::cout);
+    void run() override;
+
+  private:
+    const emp_piece_set& m_pieces;
+    const emp_strategy_generator& m_strategy;
+    std::string m_dump_file;
+    feature_options m_options;
+    std::ostream& m_out;
+};
+
 // Greedy max-placement search, printing the final board as launch_CUDA_glutton_max does.
 class feature_CUDA_glutton_max : public feature_if {
   public:
@@ -155,7 +179,8 @@ class factory_feature {
     // caller owns the returned object.  Other names throw "Unsupported feature".
     static feature_if& create_feature(const std::string& feature_name, const emp_piece_set& pieces,
                                       std::unique_ptr<emp_strategy_generator>& strategy,
-                                      const feature_options& options = {}, std::ostream& out = std::cout);
+                                      const feature_options& options = {}, std::ostream& out = std::cout,
+                                      const std::string& dump_file = "results.bin");
 };
 
 }  // namespace edge_matching_puzzle

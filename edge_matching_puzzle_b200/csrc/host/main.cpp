@@ -3,11 +3,12 @@
 //
 //   edge_matching_puzzle <definition.csv> <ressources> <feature_name> [--name=value ...]
 //
-// Feature names: CUDA_backtracker, CUDA_glutton_max.  Options the reference takes:
-//   --strategy=basic|spiral   position order of CUDA_backtracker (default basic)
+// Feature names: CUDA_backtracker, CUDA_glutton_max, new_strategy (the exhaustive
+// search with its solution file, on the GPU).  Options the reference takes:
+//   --strategy=basic|spiral   position order (CUDA_backtracker: basic, new_strategy: spiral)
+//   --dump_file=<path>        new_strategy's solution file (default results.bin)
 //   --enable_gui=...          accepted and ignored (there is no GUI here)
-//   --dump_file, --initial_situation, --hint   accepted and ignored, as the reference's
-//                             CUDA features ignore them
+//   --initial_situation, --hint   accepted and ignored
 // Settings the reference hard-codes, exposed here:
 //   --stop_at_first=true|false  --split_depth=N  --push_budget=N  --timeout_ms=N  --device=N
 // Errors print "ERROR : <what> at <file>:<line>" and exit with -1.
@@ -79,8 +80,9 @@ int main(int argc, char** argv)
         std::unique_ptr<emp_strategy_generator> strategy;
         if (named.count("strategy"))
             strategy = create_strategy_generator(named["strategy"], pieces.width, pieces.height);
+        const std::string dump_file = named.count("dump_file") ? named["dump_file"] : "results.bin";
         std::unique_ptr<feature_if> feature(
-            &factory_feature::create_feature(positional[2], pieces, strategy, options, std::cout));
+            &factory_feature::create_feature(positional[2], pieces, strategy, options, std::cout, dump_file));
         feature->run();
     } catch (emp_logic_error& e) {
         std::cout << "ERROR : " << e.what() << " at " << e.get_file() << ":" << e.get_line() << std::endl;

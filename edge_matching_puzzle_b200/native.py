@@ -81,6 +81,10 @@ class BtResult(ctypes.Structure):
     ]
 
 
+class BtSolution(ctypes.Structure):
+    _fields_ = [("node_index", ctypes.c_uint64), ("board", ctypes.c_uint32 * 256)]
+
+
 class TuneResult(ctypes.Structure):
     _fields_ = [
         ("best", BtConfig),
@@ -151,6 +155,8 @@ SIGNATURES = {
     "emp_bt_plan_subtree_counts": (ctypes.c_int32, [ctypes.c_void_p, u64p, u64p, ctypes.c_uint64]),
     "emp_bt_plan_subtree_prefix": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_uint64, u16p, ctypes.c_uint32]),
     "emp_bt_plan_destroy": (None, [ctypes.c_void_p]),
+    "emp_bt_solutions": (ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(BtConfig), ctypes.POINTER(BtSolution),
+                                          ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(BtResult)]),
     "emp_bt_autotune": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_uint32, ctypes.POINTER(BtConfig), ctypes.c_uint32,
                                          ctypes.POINTER(TuneResult)]),
     "emp_mlp_create": (ctypes.c_int32, [ctypes.c_uint64, ctypes.c_int32, ctypes.POINTER(ctypes.c_void_p)]),
@@ -266,6 +272,18 @@ def bt_count_batch(puzzles: Sequence[NativePuzzle], **kw) -> List[BtResult]:
     cfg = bt_config(**kw)
     check(load().emp_bt_count_batch(arr, len(puzzles), ctypes.byref(cfg), res))
     return list(res)
+
+
+def bt_solutions(puzzle: NativePuzzle, capacity: int = 4096, **kw):
+    """emp_bt_solutions: (found, [(node_index, board)], result) in the reference's order."""
+    out = (BtSolution * max(capacity, 1))()
+    found = ctypes.c_uint64()
+    res = BtResult()
+    cfg = bt_config(**kw)
+    check(load().emp_bt_solutions(puzzle.handle, ctypes.byref(cfg), out, capacity, ctypes.byref(found),
+                                  ctypes.byref(res)))
+    n = min(found.value, capacity)
+    return found.value, [(out[i].node_index, list(out[i].board)) for i in range(n)], res
 
 
 def bt_autotune(puzzles: Sequence[NativePuzzle], trial_ms: int = 200, **kw) -> TuneResult:

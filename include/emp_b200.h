@@ -155,6 +155,23 @@ emp_status emp_bt_count(emp_puzzle puzzle, const emp_bt_config *config, emp_bt_r
 emp_status emp_bt_count_batch(const emp_puzzle *puzzles, uint32_t count, const emp_bt_config *config,
                               emp_bt_result *results);
 
+/* One solution of the exhaustive search, placed where the reference's sequential
+ * search finds it. */
+typedef struct emp_bt_solution {
+    uint64_t node_index;         /* placements made by the sequential search up to and including this
+                                    solution: the count the reference's results.bin stores with it
+                                    (include/emp_situation_binary_dumper.h:103-117) */
+    uint32_t board[256];         /* per board position y*w+x: (piece id-1)<<2 | orientation */
+} emp_bt_solution;
+
+/* Every solution of one puzzle in the reference's order, with its node index: what
+ * emp_strategy writes to results.bin (include/emp_strategy.h:367-375).  The search runs
+ * without handing work between threads (each subtree is searched in order by one
+ * thread), so it is slower than emp_bt_count on large trees.  *found receives the
+ * number of solutions; the first min(found, capacity) are written to out. */
+emp_status emp_bt_solutions(emp_puzzle puzzle, const emp_bt_config *config, emp_bt_solution *out, uint64_t capacity,
+                            uint64_t *found, emp_bt_result *result);
+
 /* Split form of the batch call: plan (upload + prefix expansion), run (kernel
  * launch on a stream, asynchronous), results (synchronise + download). */
 typedef struct emp_bt_plan_t *emp_bt_plan;

@@ -9,7 +9,7 @@ import random
 import pytest
 
 from edge_matching_puzzle_b200 import native
-from edge_matching_puzzle_b200.puzzle import Puzzle, board_string, generate, spiral_order
+from edge_matching_puzzle_b200.puzzle import Puzzle, board_string, generate, row_major_order, spiral_order
 from oracle.oracle import OraclePuzzle
 
 pytestmark = pytest.mark.gpu
@@ -184,3 +184,40 @@ def test_stop_at_any_solution(config_counts):
     assert r0.first_found_us == 0 and not r0.has_first_solution
     assert (r0.nodes, r0.solutions) == (recs[12]["nodes"], 0)
     assert r0.status == native.EMP_OK
+
+
+def _results_bin(pz, order, solutions, total):
+    """The reference's solution file from (node_index, board) pairs."""
+    import struct
+    n = pz.width * pz.height
+    out = struct.pack("<4I", 1, pz.width, pz.height, 1)
+    for pos in order:
+        out += struct.pack("<2I", pos % pz.width, pos // pz.width)
+    field = (n - 1).bit_length() + 2
+    words = (n * field + 63) // 64
+    for node_index, board in solutions:
+        v = 0
+        for i, pos in enumerate(order):
+            v |= board[pos] << (i * field)
+        out += v.to_bytes(8 * words, "little") + struct.pack("<Q", node_index)
+    return out + struct.pack("<Q", total)
+
+
+@pytest.mark.parametrize("seed", range(8))
+def test_solution_dump_matches_oracle_results_bin(tmp_path, seed):
+    """emp_bt_solutions: every solution with the node index of the sequential search,
+    byte-identical to the oracle's results.bin (row-major and spiral orders)."""
+    rng = random.Random(7000 + seed)
+    while True:
+        w, h = rng.randint(3, 5), rng.randint(3, 5)
+        pz = generate(w, h, rng.randint(1, 3), rng.randint(2, 4), rng.randint(0, 1 << 30))
+        op = OraclePuzzle(w, h, pz.colors)
+        if op.estimate(1000) < 2e6:
+            break
+    for order in (row_major_order(w, h), spiral_order(w, h)):
+        path = str(tmp_path / "oracle.bin")
+        want, _ = op.run(order=order, results_bin=path)
+        npz = native.NativePuzzle(w, h, pz.colors, order=order)
+        found, sols, res = native.bt_solutions(npz, capacity=1 << 16, split_depth=min(4, w * h - 2))
+        assert found == want.solutions and res.nodes == want.nodes
+        assert _results_bin(pz, order, sols, res.nodes) == open(path, "rb").read()

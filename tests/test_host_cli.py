@@ -100,3 +100,18 @@ def test_backtracker_first_solution_and_totals(cli, example, reference_vectors, 
     expected = [l for l in reference_vectors["new_strategy"][name]["expected_stdout"]
                 if l.startswith(("Total situations explored", "Nb solutions"))]
     assert all(l in out for l in expected), (expected, out)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["3_3", "4_4", "5_5"])
+def test_new_strategy_results_bin_matches_reference(cli, example, reference_vectors, tmp_path, name):
+    """tests/new_strategy_<name>: the GPU search writes the reference's own results.bin
+    byte for byte (spiral order, every solution with its node index) and the totals."""
+    import base64
+    dump = tmp_path / "results.bin"
+    rc, out = run(cli, example(name), "ressources", "new_strategy", "--enable_gui=false", f"--dump_file={dump}")
+    assert rc == 0, out
+    golden = reference_vectors["new_strategy"][name]
+    assert dump.read_bytes() == base64.b64decode(golden["results_bin_b64"])
+    expected = [l for l in golden["expected_stdout"] if l.startswith(("Total situations explored", "Nb solutions"))]
+    assert all(l in out for l in expected), (expected, out)
