@@ -394,13 +394,14 @@ def run_glutton(args, rank, world, local_rank):
     print(json.dumps(out), flush=True)
 
 
-LEARN_TRAIN_SEEDS = range(1000, 1064)
+LEARN_TRAIN_SEEDS = range(1000, 1256)
 LEARN_EVAL_SEEDS = range(100, 164)
 LEARN_TIMEOUT_MS = 30000
 LEARN_WORKLOAD = ("time to a first solution of 64 seeded 8x8 puzzles (4 border / 8 interior colours, seeds "
                   "100..163), split depth 12, stop at the first solution any thread finds; plain order against "
-                  "subtrees queued best first by the network trained on the solver's solution paths of seeds "
-                  "1000..1063 (the ordering's scoring and sort are counted in its time)")
+                  "subtrees queued best first by the network trained on the solver's solution paths (levels "
+                  "below the split depth) of seeds 1000..1255 (the ordering's scoring and sort are counted in "
+                  "its time)")
 
 
 def run_learned(args, rank, world, local_rank):
@@ -421,7 +422,7 @@ def run_learned(args, rank, world, local_rank):
             train_h.append(h)
             boards.append(list(r.first_solution))
     model = native.Mlp(seed=1, device=local_rank)
-    rep = model.train(train_h, boards, epochs=args.learn_epochs, batch=2048, learning_rate=1e-3)
+    rep = model.train(train_h, boards, epochs=args.learn_epochs, batch=1024, learning_rate=1e-3, max_level=DEPTH)
     train_s = time.perf_counter() - t_train0
     rows = []
     for s in LEARN_EVAL_SEEDS:

@@ -347,7 +347,8 @@ extern "C" emp_status emp_mlp_train(emp_mlp model, const emp_puzzle* puzzles, ui
     std::vector<emp::FeatItem> items;
     std::vector<float> labels;
     // levels past 63 are left out: the candidate step replays prefixes of at most 64 levels
-    for (uint32_t l = 1; l + 1 < max_n && l < 64; ++l) {
+    const uint32_t level_limit = cfg.max_level ? std::min<uint32_t>(cfg.max_level, 64u) : 64u;
+    for (uint32_t l = 1; l + 1 < max_n && l < level_limit; ++l) {
         std::vector<uint16_t> parents;
         std::vector<uint32_t> ppz;
         for (uint32_t i = 0; i < P; ++i)

@@ -97,7 +97,7 @@ class TuneResult(ctypes.Structure):
 
 class MlpTrainConfig(ctypes.Structure):
     _fields_ = [("epochs", ctypes.c_uint32), ("batch", ctypes.c_uint32), ("learning_rate", ctypes.c_float),
-                ("seed", ctypes.c_uint32), ("reserved", ctypes.c_uint32 * 4)]
+                ("seed", ctypes.c_uint32), ("max_level", ctypes.c_uint32), ("reserved", ctypes.c_uint32 * 3)]
 
 
 class MlpTrainReport(ctypes.Structure):
@@ -362,13 +362,14 @@ class Mlp:
         return loss.value, grads
 
     def train(self, puzzles: Sequence[NativePuzzle], solutions, epochs: int = 0, batch: int = 0,
-              learning_rate: float = 0.0, seed: int = 1) -> MlpTrainReport:
+              learning_rate: float = 0.0, seed: int = 1, max_level: int = 0) -> MlpTrainReport:
         """solutions: one emp_bt_result.first_solution board (256 values) per puzzle."""
         import numpy as np
         arr = (ctypes.c_void_p * len(puzzles))(*[p.handle for p in puzzles])
         boards = np.ascontiguousarray(solutions, dtype=np.uint32).reshape(len(puzzles), 256)
         cfg = MlpTrainConfig()
         cfg.epochs, cfg.batch, cfg.learning_rate, cfg.seed = epochs, batch, learning_rate, seed
+        cfg.max_level = max_level
         rep = MlpTrainReport()
         check(load().emp_mlp_train(self.handle, arr, len(puzzles), boards.ctypes.data, ctypes.byref(cfg),
                                    ctypes.byref(rep)))

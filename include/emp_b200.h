@@ -263,7 +263,9 @@ typedef struct emp_mlp_train_config {
     uint32_t batch;              /* rows per step; 0 = 2048 */
     float learning_rate;         /* Adam step size; 0 = 1e-3 */
     uint32_t seed;               /* shuffling */
-    uint32_t reserved[4];
+    uint32_t max_level;          /* train on levels below this one only (the levels an ordered plan
+                                    scores: its split depth); 0 = every level */
+    uint32_t reserved[3];
 } emp_mlp_train_config;
 
 typedef struct emp_mlp_train_report {
