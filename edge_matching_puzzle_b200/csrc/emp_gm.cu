@@ -35,6 +35,7 @@ namespace {
 
 constexpr int kThreads = 1024;
 constexpr unsigned kFull = 0xFFFFFFFFu;
+constexpr uint64_t kBarrierWaitNs = 5000000000ull;  // 5 s: far beyond one validity pass
 
 struct GmSmem {
     uint32_t X[256][32];       // infos of the current level
@@ -48,6 +49,7 @@ struct GmSmem {
     uint8_t pieces[256][4];
     uint32_t position_index[256];
     uint32_t info_index[256];
+    uint32_t played[256];      // this block's copy of the played stack
     uint32_t avail[8];
     unsigned long long warp_key[32];
     uint32_t warp_order[32];
@@ -276,12 +278,13 @@ __device__ void store_level(const GmSmem& sm, const GmLaunch& P, uint32_t level,
 }
 
 // CUDA_glutton_max_stack::pop (thread 0); returns the restored info index.
-__device__ uint32_t pop_state(GmSmem& sm, GmState* st, uint32_t S)
+// `owner` (the block that keeps the global search record) also updates it.
+__device__ uint32_t pop_state(GmSmem& sm, GmState* st, uint32_t S, bool owner)
 {
     const uint32_t level = sm.level;
     const uint32_t last = S - level;
     const uint32_t info = sm.position_index[last];
-    const uint32_t played = st->played[level - 1];
+    const uint32_t played = sm.played[level - 1];
     const uint32_t pos = played & 0xFFu;
     sm.level = level - 1;
     const uint32_t piece = (played >> 8) & 0xFFu;
@@ -294,21 +297,26 @@ __device__ uint32_t pop_state(GmSmem& sm, GmState* st, uint32_t S)
     t = sm.position_index[info];
     sm.position_index[info] = sm.position_index[last];
     sm.position_index[last] = t;
-    st->pops++;
+    if (owner) st->pops++;
     return info;
 }
 
 // CUDA_glutton_max_stack::push (thread 0).
-__device__ void push_state(GmSmem& sm, GmState* st, uint32_t S, uint32_t info, uint32_t pos, uint32_t piece, uint32_t o)
+__device__ void push_state(GmSmem& sm, GmState* st, uint32_t S, uint32_t info, uint32_t pos, uint32_t piece, uint32_t o,
+                           bool owner)
 {
     const uint32_t level = sm.level;
-    st->played[level] = (o << 16) | (piece << 8) | pos;
+    sm.played[level] = (o << 16) | (piece << 8) | pos;
     sm.avail[piece >> 5] &= ~(1u << (piece & 31));
     const uint32_t nl = level + 1;
     sm.level = nl;
-    if (nl > st->max) {
-        for (uint32_t l = 0; l <= st->max && l < S; ++l) st->max_played[l] = st->played[l];
-        st->max = nl;
+    if (owner) {
+        st->played[level] = sm.played[level];
+        if (nl > st->max) {
+            for (uint32_t l = 0; l <= st->max && l < S; ++l) st->max_played[l] = sm.played[l];
+            st->max = nl;
+        }
+        st->pushes++;
     }
     const uint32_t last = S - nl;
     const uint32_t last_pos = sm.position_index[last];
@@ -319,9 +327,45 @@ __device__ void push_state(GmSmem& sm, GmState* st, uint32_t S, uint32_t info, u
     t = sm.position_index[info];
     sm.position_index[info] = sm.position_index[last];
     sm.position_index[last] = t;
-    st->pushes++;
 }
 
+// Grid barrier of the cooperative launch (all blocks are resident).  The wait is
+// bounded: past the deadline the block flags an error and the barrier reports it.
+__device__ bool grid_sync(GmGrid* g, uint32_t nblocks)
+{
+    __syncthreads();
+    __shared__ uint32_t ok_s;
+    if (threadIdx.x == 0) {
+        uint32_t ok = 1;
+        const uint32_t gen = *(volatile uint32_t*)&g->bar_gen;
+        __threadfence();
+        if (atomicAdd(&g->bar_count, 1u) == nblocks - 1) {
+            g->bar_count = 0;
+            __threadfence();
+            atomicAdd(&g->bar_gen, 1u);
+        } else {
+            const uint64_t deadline = global_ns() + kBarrierWaitNs;
+            while (*(volatile uint32_t*)&g->bar_gen == gen) {
+                if (*(volatile int*)&g->error || global_ns() > deadline) {
+                    atomicExch(&g->error, 1);
+                    ok = 0;
+                    break;
+                }
+            }
+        }
+        __threadfence();
+        ok_s = ok;
+    }
+    __syncthreads();
+    return ok_s != 0;
+}
+
+// One glutton max search.  GRID = false: one block does everything.  GRID = true:
+// every block of a cooperative launch keeps a copy of the level and makes the same
+// decisions; the candidate trials of each validity pass are shared out over the warps
+// of all blocks through global memory (triple-buffered per pass, one grid barrier per
+// pass), and block 0 keeps the global search record.
+template <bool GRID>
 __global__ void __launch_bounds__(kThreads, 1) gm_kernel(GmLaunch P)
 {
     extern __shared__ __align__(16) unsigned char gm_raw[];
@@ -329,11 +373,17 @@ __global__ void __launch_bounds__(kThreads, 1) gm_kernel(GmLaunch P)
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint32_t S = P.n;
     GmState* st = P.state;
+    GmGrid* g = P.grid;
+    const bool owner = !GRID || blockIdx.x == 0;
+    const uint32_t nblocks = gridDim.x;
+    uint32_t pass_no = 0;  // grid mode: passes so far (selects the exchange buffer)
+    bool grid_failed = false;
     for (uint32_t k = tid; k < 256 * 4; k += kThreads) sm.pieces[k >> 2][k & 3] = P.pieces[k];
     for (uint32_t k = tid; k < P.ncolours * 4 * 32; k += kThreads) (&sm.cc[0][0][0])[k] = P.cc[k];
     for (uint32_t k = tid; k < 256; k += kThreads) {
         sm.position_index[k] = st->position_index[k];
         sm.info_index[k] = st->info_index[k];
+        sm.played[k] = st->played[k];
     }
     if (tid < 8) sm.avail[tid] = st->avail[tid];
     if (tid == 0) {
@@ -350,11 +400,20 @@ __global__ void __launch_bounds__(kThreads, 1) gm_kernel(GmLaunch P)
     for (;;) {
         const uint32_t level = sm.level;
         if (level >= S) break;  // full board (level == S) or exhausted (wrapped below 0)
-        if (tid == 0) {
-            if ((P.push_budget && st->pushes >= P.push_budget) ||
-                (P.placement_budget && st->trials + st->pushes >= P.placement_budget) ||
-                (deadline && global_ns() > deadline))
-                sm.stop = 1;
+        if (owner && tid == 0) {
+            const bool stop = (P.push_budget && st->pushes >= P.push_budget) ||
+                              (P.placement_budget && st->trials + st->pushes >= P.placement_budget) ||
+                              (deadline && global_ns() > deadline);
+            sm.stop = stop;
+            if (GRID) g->stop = stop;
+        }
+        if (GRID) {
+            // every block follows block 0's decision
+            if (!grid_sync(g, nblocks)) {
+                grid_failed = true;
+                break;
+            }
+            if (tid == 0) sm.stop = *(volatile uint32_t*)&g->stop;
         }
         __syncthreads();
         if (sm.stop) break;
@@ -366,7 +425,7 @@ __global__ void __launch_bounds__(kThreads, 1) gm_kernel(GmLaunch P)
                 __syncthreads();
                 if (tid == 0) {
                     if (level == 0) sm.level = ~0u;
-                    else sm.pop_index = pop_state(sm, st, S);
+                    else sm.pop_index = pop_state(sm, st, S, owner);
                     sm.new_level = 0;
                 }
                 __syncthreads();
@@ -375,7 +434,7 @@ __global__ void __launch_bounds__(kThreads, 1) gm_kernel(GmLaunch P)
                 continue;
             }
         }
-        if (tid == 0) st->levels++;
+        if (owner && tid == 0) st->levels++;
         // ---- validity fixpoint and scores ----
         bool failed = false;
         for (;;) {
@@ -384,11 +443,14 @@ __global__ void __launch_bounds__(kThreads, 1) gm_kernel(GmLaunch P)
                 failed = true;
                 break;
             }
-            for (uint32_t k = tid; k < nb * 32; k += kThreads) sm.inval[k >> 5][k & 31] = 0;
+            const uint32_t buf = pass_no % 3;
+            if (!GRID) {
+                for (uint32_t k = tid; k < nb * 32; k += kThreads) sm.inval[k >> 5][k & 31] = 0;
+            }
             if (tid == 0) {
                 sm.any_invalid = 0;
                 sm.next_info = 0;
-                st->passes++;
+                if (owner) st->passes++;
             }
             __syncthreads();
             unsigned long long best_key = 0;
@@ -396,7 +458,7 @@ __global__ void __launch_bounds__(kThreads, 1) gm_kernel(GmLaunch P)
             const bool last_level = level == S - 1;
             for (;;) {
                 uint32_t i = 0;
-                if (lane == 0) i = atomicAdd(&sm.next_info, 1u);
+                if (lane == 0) i = GRID ? atomicAdd(&g->next_info[buf], 1u) : atomicAdd(&sm.next_info, 1u);
                 i = __shfl_sync(kFull, i, 0);
                 if (i >= nb) break;
                 for (uint32_t w = 0; w < 32; ++w) {
@@ -409,8 +471,13 @@ __global__ void __launch_bounds__(kThreads, 1) gm_kernel(GmLaunch P)
                         const uint32_t order = (i << 10) | (w << 5) | b;
                         if (!t.valid) {
                             if (lane == 0) {
-                                atomicOr(&sm.inval[i][w], 1u << b);
-                                sm.any_invalid = 1;
+                                if (GRID) {
+                                    atomicOr(&g->inval[buf][i][w], 1u << b);
+                                    g->any_invalid[buf] = 1;
+                                } else {
+                                    atomicOr(&sm.inval[i][w], 1u << b);
+                                    sm.any_invalid = 1;
+                                }
                             }
                             continue;
                         }
@@ -432,43 +499,78 @@ __global__ void __launch_bounds__(kThreads, 1) gm_kernel(GmLaunch P)
                 sm.warp_trials[warp] = trials;
             }
             __syncthreads();
-            if (!sm.any_invalid) {
+            // this block's best (a strict total order: any reduction order gives the same result)
+            if (tid == 0) {
+                unsigned long long k0 = 0;
+                uint32_t o0 = ~0u;
+                unsigned long long tr = 0;
+                for (int w = 0; w < kThreads / 32; ++w) {
+                    tr += sm.warp_trials[w];
+                    const uint32_t o = sm.warp_order[w];
+                    if (o == ~0u) continue;
+                    const unsigned long long k = sm.warp_key[w];
+                    if (o0 == ~0u || (last_level ? o > o0 : (k > k0 || (k == k0 && o < o0)))) {
+                        k0 = k;
+                        o0 = o;
+                    }
+                }
+                if (GRID) {
+                    atomicAdd(&st->trials, tr);
+                    g->blk_key[buf][blockIdx.x] = k0;
+                    g->blk_order[buf][blockIdx.x] = o0;
+                } else {
+                    st->trials += tr;
+                    sm.best_order = o0;
+                }
+            }
+            if (GRID) {
+                if (!grid_sync(g, nblocks)) {
+                    grid_failed = true;
+                    break;
+                }
+                // the buffer of the pass before last is free again: block 0 clears it
+                if (blockIdx.x == 0) {
+                    const uint32_t old = (pass_no + 2) % 3;
+                    for (uint32_t k = tid; k < S * 32; k += kThreads) (&g->inval[old][0][0])[k] = 0;
+                    if (tid == 0) {
+                        g->any_invalid[old] = 0;
+                        g->next_info[old] = 0;
+                    }
+                }
                 if (tid == 0) {
+                    sm.any_invalid = *(volatile uint32_t*)&g->any_invalid[buf];
                     unsigned long long k0 = 0;
                     uint32_t o0 = ~0u;
-                    unsigned long long tr = 0;
-                    for (int w = 0; w < kThreads / 32; ++w) {
-                        tr += sm.warp_trials[w];
-                        const uint32_t o = sm.warp_order[w];
+                    for (uint32_t b2 = 0; b2 < nblocks; ++b2) {
+                        const uint32_t o = *(volatile uint32_t*)&g->blk_order[buf][b2];
                         if (o == ~0u) continue;
-                        const unsigned long long k = sm.warp_key[w];
-                        const bool better =
-                            o0 == ~0u || (last_level ? o > o0 : (k > k0 || (k == k0 && o < o0)));
-                        if (better) {
+                        const unsigned long long k = *(volatile unsigned long long*)&g->blk_key[buf][b2];
+                        if (o0 == ~0u || (last_level ? o > o0 : (k > k0 || (k == k0 && o < o0)))) {
                             k0 = k;
                             o0 = o;
                         }
                     }
                     sm.best_order = o0;
-                    st->trials += tr;
                 }
-                __syncthreads();
-                break;
+                ++pass_no;
             }
-            if (tid == 0) {
-                unsigned long long tr = 0;
-                for (int w = 0; w < kThreads / 32; ++w) tr += sm.warp_trials[w];
-                st->trials += tr;
+            __syncthreads();
+            if (!sm.any_invalid) break;
+            if (GRID) {
+                for (uint32_t k = tid; k < nb * 32; k += kThreads)
+                    sm.X[k >> 5][k & 31] &= ~(*(volatile uint32_t*)&g->inval[buf][k >> 5][k & 31]);
+            } else {
+                for (uint32_t k = tid; k < nb * 32; k += kThreads) sm.X[k >> 5][k & 31] &= ~sm.inval[k >> 5][k & 31];
             }
-            for (uint32_t k = tid; k < nb * 32; k += kThreads) sm.X[k >> 5][k & 31] &= ~sm.inval[k >> 5][k & 31];
             __syncthreads();
         }
+        if (grid_failed) break;
         if (failed || sm.best_order == ~0u) {
             // remove_invalid_transitions failed or no candidate: pop
             __syncthreads();
             if (tid == 0) {
                 if (level == 0) sm.level = ~0u;
-                else sm.pop_index = pop_state(sm, st, S);
+                else sm.pop_index = pop_state(sm, st, S, owner);
                 sm.new_level = 0;
             }
             __syncthreads();
@@ -482,7 +584,10 @@ __global__ void __launch_bounds__(kThreads, 1) gm_kernel(GmLaunch P)
         const uint32_t pos = sm.position_index[bi];
         if (tid == 0) sm.X[bi][bw] &= ~(1u << bb);
         __syncthreads();
-        store_level(sm, P, level, tid);  // the level keeps its remaining candidates for a later pop
+        // the level keeps its remaining candidates for a later pop (in grid mode every
+        // block writes the same values and reads back only its own writes)
+        store_level(sm, P, level, tid);
+        __threadfence_block();
         const uint32_t pm_word = ~(0xFu << (4 * (bb / 4)));
         // the next level moves the last info into the chosen slot; an empty
         // result there stops the reference's apply before its push
@@ -503,20 +608,20 @@ __global__ void __launch_bounds__(kThreads, 1) gm_kernel(GmLaunch P)
             else sm.X[j][w] &= m;
         }
         __syncthreads();
-        if (tid == 0) push_state(sm, st, S, bi, pos, piece, o);
+        if (tid == 0) push_state(sm, st, S, bi, pos, piece, o, owner);
         __syncthreads();
         // colour constraints of the placed piece on its free neighbours
         if (warp == 0) {
             const uint32_t nl = sm.level, nbn = S - nl;
             const int off[4] = {-static_cast<int>(P.width), 1, static_cast<int>(P.width), -1};
             bool invalid = false;
-            for (uint32_t s = 0; s < 4 && !invalid; ++s) {
-                const uint32_t col = sm.pieces[piece][(s + o) & 3u];
+            for (uint32_t s2 = 0; s2 < 4 && !invalid; ++s2) {
+                const uint32_t col = sm.pieces[piece][(s2 + o) & 3u];
                 if (!col) continue;
-                const uint32_t npos = static_cast<uint32_t>(static_cast<int>(pos) + off[s]);
+                const uint32_t npos = static_cast<uint32_t>(static_cast<int>(pos) + off[s2]);
                 const uint32_t j = sm.info_index[npos];
                 if (j >= nbn) continue;
-                const uint32_t r = sm.X[j][lane] & sm.cc[col - 1][s][lane];
+                const uint32_t r = sm.X[j][lane] & sm.cc[col - 1][s2][lane];
                 if (!__any_sync(kFull, r)) {
                     invalid = true;
                     break;
@@ -528,21 +633,22 @@ __global__ void __launch_bounds__(kThreads, 1) gm_kernel(GmLaunch P)
         __syncthreads();
         if (sm.apply_failed) {
             __syncthreads();
-            if (tid == 0) pop_state(sm, st, S);
+            if (tid == 0) pop_state(sm, st, S, owner);
             __syncthreads();
             load_level(sm, P, sm.level, tid);
         }
         if (tid == 0) sm.new_level = 1;
         __syncthreads();
     }
-    // write the search state back
+    // write the search state back (the owner block)
     __syncthreads();
+    if (!owner) return;
     if (tid == 0) {
         const uint32_t level = sm.level;
         st->level = level;
         st->new_level = sm.new_level;
         st->pop_index = sm.pop_index;
-        st->status = level == S ? 0 : (level > S ? 2 : 1);
+        st->status = grid_failed ? 3 : (level == S ? 0 : (level > S ? 2 : 1));
     }
     if (sm.level < S) store_level(sm, P, sm.level, tid);
     for (uint32_t k = tid; k < 256; k += kThreads) {
@@ -559,10 +665,31 @@ size_t gm_smem_bytes() { return sizeof(GmSmem); }
 cudaError_t launch_gm(const GmLaunch& P, cudaStream_t stream)
 {
     const size_t smem = sizeof(GmSmem);
-    cudaError_t e = cudaFuncSetAttribute(gm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    cudaError_t e = cudaFuncSetAttribute(gm_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(smem));
     if (e != cudaSuccess) return e;
-    gm_kernel<<<1, kThreads, smem, stream>>>(P);
+    gm_kernel<false><<<1, kThreads, smem, stream>>>(P);
     return cudaGetLastError();
+}
+
+cudaError_t launch_gm_grid(const GmLaunch& P, uint32_t blocks, cudaStream_t stream)
+{
+    const size_t smem = sizeof(GmSmem);
+    cudaError_t e = cudaFuncSetAttribute(gm_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(smem));
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gm_kernel<true>, kThreads, smem);
+    if (e != cudaSuccess) return e;
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (per_sm < 1 || blocks > static_cast<uint32_t>(per_sm * sms) || blocks > kMaxGridBlocks || !blocks)
+        return cudaErrorCooperativeLaunchTooLarge;
+    GmLaunch copy = P;
+    void* args[] = {&copy};
+    return cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(&gm_kernel<true>), dim3(blocks), dim3(kThreads),
+                                       args, smem, stream);
 }
 
 }  // namespace emp

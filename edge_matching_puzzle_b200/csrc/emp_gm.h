@@ -11,7 +11,8 @@ namespace emp {
 struct GmState {
     uint32_t level;              // pieces placed (the reference's m_level)
     uint32_t max;                // best level reached (m_max)
-    int32_t status;              // 0 full board, 1 budget or deadline reached, 2 search exhausted
+    int32_t status;              // 0 full board, 1 budget or deadline reached, 2 search exhausted,
+                                 // 3 multi-block search stopped by a barrier timeout
     uint32_t new_level;          // the kernel loop's l_new_level
     uint32_t pop_index;          // info index returned by the last pop
     uint32_t pad[3];
@@ -27,6 +28,19 @@ struct GmState {
     uint32_t avail[8];           // piece availability bits
 };
 
+// Exchange area of the multi-block search (one per search, global memory).
+constexpr uint32_t kMaxGridBlocks = 256;
+struct GmGrid {
+    uint32_t bar_count, bar_gen;  // grid barrier
+    int error;                    // a barrier wait ran out of time
+    uint32_t stop;                // block 0's decision at the top of a level
+    uint32_t any_invalid[3];      // per pass buffer (pass number mod 3)
+    uint32_t next_info[3];
+    uint32_t inval[3][256][32];
+    unsigned long long blk_key[3][kMaxGridBlocks];
+    uint32_t blk_order[3][kMaxGridBlocks];
+};
+
 struct GmLaunch {
     const uint8_t* pieces;       // [256][4] colours N,E,S,W per piece index
     const uint32_t* cc;          // [ncolours][4][32] colour constraints
@@ -36,9 +50,12 @@ struct GmLaunch {
     unsigned long long push_budget;   // stop after this many pushes (0: none)
     unsigned long long placement_budget;  // stop once trials + pushes reach this (0: none)
     unsigned long long timeout_ns;    // stop after this long (0: none)
+    GmGrid* grid = nullptr;           // multi-block search: the exchange area (zeroed before the launch)
 };
 
 size_t gm_smem_bytes();
 cudaError_t launch_gm(const GmLaunch& P, cudaStream_t stream);
+// The same search over `blocks` blocks of a cooperative launch (at most one per SM).
+cudaError_t launch_gm_grid(const GmLaunch& P, uint32_t blocks, cudaStream_t stream);
 
 }  // namespace emp

@@ -5,6 +5,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <chrono>
 #include <cstring>
 #include <mutex>
@@ -114,8 +115,15 @@ extern "C" emp_status emp_glutton_max(emp_puzzle puzzle, const emp_gm_config* co
         st.max_played[i] = 0xFFFFFFFFu;
     }
     for (uint32_t i = 0; i < m.n; ++i) st.avail[i >> 5] |= 1u << (i & 31);
-    DeviceBuffer d_pieces, d_cc, d_infos, d_state;
+    DeviceBuffer d_pieces, d_cc, d_infos, d_state, d_grid;
     const size_t tri = static_cast<size_t>(S) * (S + 1) / 2;
+    uint32_t blocks = cfg.blocks;
+    if (!blocks) blocks = static_cast<uint32_t>(prop.multiProcessorCount);
+    blocks = std::min<uint32_t>(blocks, std::min<uint32_t>(emp::kMaxGridBlocks, prop.multiProcessorCount));
+    if (blocks > 1) {
+        CUDA_TRY(d_grid.alloc(sizeof(emp::GmGrid)));
+        CUDA_TRY(cudaMemset(d_grid.p, 0, sizeof(emp::GmGrid)));
+    }
     CUDA_TRY(d_pieces.alloc(pieces.size()));
     CUDA_TRY(d_cc.alloc(sizeof(uint32_t) * std::max<size_t>(cc.size(), 1)));
     CUDA_TRY(d_infos.alloc(sizeof(uint32_t) * 32 * tri));
@@ -134,6 +142,7 @@ extern "C" emp_status emp_glutton_max(emp_puzzle puzzle, const emp_gm_config* co
     P.ncolours = m.border_id;
     P.push_budget = cfg.push_budget;
     P.placement_budget = cfg.placement_budget;
+    P.grid = blocks > 1 ? d_grid.as<emp::GmGrid>() : nullptr;
     // without a caller limit the search still stops after an hour on the device
     const unsigned long long ms_limit = cfg.timeout_ms ? cfg.timeout_ms : 3600000ull;
     P.timeout_ns = ms_limit * 1000000ull;
@@ -141,7 +150,7 @@ extern "C" emp_status emp_glutton_max(emp_puzzle puzzle, const emp_gm_config* co
     CUDA_TRY(cudaEventCreate(&e0));
     CUDA_TRY(cudaEventCreate(&e1));
     CUDA_TRY(cudaEventRecord(e0));
-    cudaError_t le = emp::launch_gm(P, nullptr);
+    cudaError_t le = blocks > 1 ? emp::launch_gm_grid(P, blocks, nullptr) : emp::launch_gm(P, nullptr);
     if (le != cudaSuccess) {
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
@@ -166,6 +175,7 @@ extern "C" emp_status emp_glutton_max(emp_puzzle puzzle, const emp_gm_config* co
     result->passes = st.passes;
     result->levels = st.levels;
     result->kernel_ms = ms;
+    if (st.status == 3) return fail(EMP_ERR_CUDA, "glutton max: a grid barrier of the multi-block search timed out");
     return st.status == 1 ? EMP_INCOMPLETE : EMP_OK;
 }
 

@@ -113,7 +113,7 @@ MLP_PARAMS = 256 * 512 + 256 + 256 * 256 + 256 + 256 + 1
 
 class GmConfig(ctypes.Structure):
     _fields_ = [("push_budget", ctypes.c_uint64), ("timeout_ms", ctypes.c_uint32), ("device", ctypes.c_int32),
-                ("placement_budget", ctypes.c_uint64), ("reserved", ctypes.c_uint32 * 6)]
+                ("placement_budget", ctypes.c_uint64), ("blocks", ctypes.c_uint32), ("reserved", ctypes.c_uint32 * 5)]
 
 
 class GmResult(ctypes.Structure):
@@ -397,9 +397,10 @@ def config_dict(cfg: BtConfig) -> dict:
 
 
 def glutton_max(puzzle: NativePuzzle, push_budget: int = 0, timeout_ms: int = 0, device: int = -1,
-                placement_budget: int = 0) -> GmResult:
+                placement_budget: int = 0, blocks: int = 0) -> GmResult:
     cfg = GmConfig()
     cfg.push_budget = push_budget
+    cfg.blocks = blocks
     cfg.placement_budget = placement_budget
     cfg.timeout_ms = timeout_ms
     cfg.device = device

@@ -301,7 +301,10 @@ typedef struct emp_gm_config {
     uint64_t placement_budget;   /* stop at the first level that starts with at least this many
                                     placements done (candidate trial evaluations + committed
                                     placements, the kernel's own count); 0 = none */
-    uint32_t reserved[6];
+    uint32_t blocks;             /* blocks of the search, at most one per SM: every block keeps a copy
+                                    of the level and the trials of each validity pass are shared out
+                                    over all of them; 0 = one per SM, 1 = a single block */
+    uint32_t reserved[5];
 } emp_gm_config;
 
 typedef struct emp_gm_result {

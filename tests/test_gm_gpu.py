@@ -39,10 +39,10 @@ def test_reference_glutton_boards(reference_vectors, name):
     assert board_string(pz.width, pz.height, list(r.final_board)) == reference_vectors["glutton_max"][name][-1]
 
 
-def _compare(pz, push_budget=0):
+def _compare(pz, push_budget=0, blocks=0):
     want = OraclePuzzle(pz.width, pz.height, pz.colors).glutton(push_budget=push_budget)
     got = native.glutton_max(native.NativePuzzle(pz.width, pz.height, pz.colors), push_budget=push_budget,
-                             timeout_ms=60000)
+                             timeout_ms=60000, blocks=blocks)
     assert (got.status, got.max_level, got.pushes, got.pops, got.levels) == \
         (want.status, want.max_level, want.pushes, want.pops, want.levels_evaluated)
     cells, best = _boards(pz, want)
@@ -51,17 +51,33 @@ def _compare(pz, push_budget=0):
     assert [c if c != 0xFFFFFFFF else -1 for c in list(got.best_board)[: pz.nb_pieces]] == best
 
 
+# blocks: 1 = one block, 0 = one block per SM (the trials of each pass shared over the grid)
+@pytest.mark.parametrize("blocks", [1, 0])
 @pytest.mark.parametrize("seed", range(12))
-def test_random_puzzles_full_search(seed):
+def test_random_puzzles_full_search(seed, blocks):
     rng = random.Random(500 + seed)
     w, h = rng.randint(3, 5), rng.randint(3, 5)
-    _compare(generate(w, h, rng.randint(2, 3), rng.randint(3, 6), seed))
+    _compare(generate(w, h, rng.randint(2, 3), rng.randint(3, 6), seed), blocks=blocks)
 
 
+@pytest.mark.parametrize("blocks", [1, 0])
 @pytest.mark.parametrize("seed,budget", [(0, 10), (1, 40), (2, 100)])
-def test_push_budget_trajectory(seed, budget):
+def test_push_budget_trajectory(seed, budget, blocks):
     """Bounded searches on larger puzzles stop at the same point with the same best board."""
-    _compare(generate(8, 8, 4, 8, seed), push_budget=budget)
+    _compare(generate(8, 8, 4, 8, seed), push_budget=budget, blocks=blocks)
+
+
+def test_grid_and_single_block_agree_on_16x16():
+    """The first levels of the 16x16 search: the multi-block search takes the single
+    block's trajectory (same pushes, pops, boards and trial count)."""
+    pz = generate(16, 16, 5, 17, 7)
+    h = native.NativePuzzle(16, 16, pz.colors)
+    one = native.glutton_max(h, push_budget=40, timeout_ms=120000, blocks=1)
+    grid = native.glutton_max(h, push_budget=40, timeout_ms=120000, blocks=0)
+    for f in ("status", "max_level", "level", "pushes", "pops", "levels", "passes", "trials"):
+        assert getattr(one, f) == getattr(grid, f), f
+    assert list(one.best_board) == list(grid.best_board)
+    assert list(one.final_board) == list(grid.final_board)
 
 
 def test_placement_budget_stops_the_search():
