@@ -457,13 +457,13 @@ __global__ void __launch_bounds__(kThreads, 1) gm_kernel(GmLaunch P)
             uint32_t best_order = ~0u, trials = 0;
             const bool last_level = level == S - 1;
             for (;;) {
-                // work unit: 4 words (32 pieces) of one free position's info
+                // work unit: one word (8 pieces x 4 orientations) of one free position's info
                 uint32_t u = 0;
                 if (lane == 0) u = GRID ? atomicAdd(&g->next_info[buf], 1u) : atomicAdd(&sm.next_info, 1u);
                 u = __shfl_sync(kFull, u, 0);
-                const uint32_t i = u >> 3;
+                const uint32_t i = u >> 5;
                 if (i >= nb) break;
-                for (uint32_t w = (u & 7u) * 4; w < (u & 7u) * 4 + 4; ++w) {
+                for (uint32_t w = u & 31u; w == (u & 31u); ++w) {
                     uint32_t word = sm.X[i][w];
                     while (word) {
                         const uint32_t b = __ffs(word) - 1;
