@@ -20,8 +20,10 @@
 //    neighbours & availability;
 //  * a level plan for a position order (row-major "basic" or spiral).
 //
-// Candidate bit t = (kind_index << 2) | orientation, stored in 32-bit words:
-// word t >> 5, bit t & 31, i.e. one nibble per piece (8 pieces per word).
+// Candidate bit t = (kind_index << 2) | orientation, one nibble per piece.  The
+// host model keeps 32-bit words (word t >> 5, bit t & 31: 8 pieces per word); the
+// device tables (DeviceTables below) store the same bits in 64-bit words (word
+// t >> 6, bit t & 63: 16 pieces per word).
 #pragma once
 
 #include <array>
