@@ -128,6 +128,31 @@ def test_8x8_subtree_parity_sample():  # noqa: D103
     assert res.nodes == sum(nodes) and res.solutions == sum(sols)
 
 
+def test_8x8_largest_seed_subtree_sample():
+    """Seed 13, the largest workload tree (1.5e13 placements, beyond a CPU count here):
+    per-subtree counts of a spread-out sample of its depth-12 subtrees against the oracle."""
+    pz = generate(8, 8, 4, 8, 13)
+    npz = native.NativePuzzle(8, 8, pz.colors)
+    op = OraclePuzzle(8, 8, pz.colors)
+    depth = 12
+    plan = native.BtPlan([npz], split_depth=depth, keep_subtree_counts=1, timeout_ms=120000)
+    total = plan.subtrees()
+    count, _, _, _ = op.expand(depth, max_prefixes=1 << 40)
+    assert total == count
+    sample = 600
+    stride = total // sample
+    plan.select(3, stride, sample)
+    plan.run()
+    res = plan.results()[0]
+    assert res.status == native.EMP_OK
+    nodes, sols = plan.subtree_counts(sample)
+    for i in range(0, sample, 10):
+        prefix = plan.subtree_prefix(i, depth)
+        want_n, want_s, _ = op.subtree(prefix)
+        assert (nodes[i], sols[i]) == (want_n, want_s), i
+    assert res.nodes == sum(nodes) and res.solutions == sum(sols)
+
+
 def test_8x8_full_count_against_cpu_golden(config_counts):
     """Whole exhaustive count of an 8x8 workload seed equals the CPU oracle's count."""
     recs = [r for r in config_counts["records"] if r["config"] == "8x8"]
