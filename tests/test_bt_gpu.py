@@ -153,10 +153,12 @@ def test_8x8_largest_seed_subtree_sample():
     assert res.nodes == sum(nodes) and res.solutions == sum(sols)
 
 
-def test_8x8_full_count_against_cpu_golden(config_counts):
-    """Whole exhaustive count of an 8x8 workload seed equals the CPU oracle's count."""
-    recs = [r for r in config_counts["records"] if r["config"] == "8x8"]
-    rec = min(recs, key=lambda r: r["nodes"])
+@pytest.mark.parametrize("rank", range(5))
+def test_8x8_full_count_against_cpu_golden(config_counts, rank):
+    """Whole exhaustive count of an 8x8 workload seed (the five smallest trees, 3.8e9 to
+    4.8e10 placements) equals the CPU oracle's count."""
+    recs = sorted((r for r in config_counts["records"] if r["config"] == "8x8"), key=lambda r: r["nodes"])
+    rec = recs[rank]
     pz = generate(8, 8, 4, 8, rec["seed"])
     r = native.bt_count(native.NativePuzzle(8, 8, pz.colors), split_depth=12, timeout_ms=60000)
     assert r.status == native.EMP_OK
