@@ -115,3 +115,12 @@ def test_new_strategy_results_bin_matches_reference(cli, example, reference_vect
     assert dump.read_bytes() == base64.b64decode(golden["results_bin_b64"])
     expected = [l for l in golden["expected_stdout"] if l.startswith(("Total situations explored", "Nb solutions"))]
     assert all(l in out for l in expected), (expected, out)
+
+
+def test_new_strategy_reports_errors_like_the_other_features(cli, tmp_path, reference_vectors):
+    """A bad order for new_strategy is refused before any search, with the ERROR line."""
+    path = tmp_path / "3_3.txt"
+    path.write_text(reference_vectors["puzzles"]["3_3"])
+    rc, out = run(cli, str(path), "ressources", "new_strategy", "--strategy=zigzag", f"--dump_file={tmp_path / 'r.bin'}")
+    assert rc == 255 and 'Unsupported strategy "zigzag"' in out[-1]
+    assert not (tmp_path / "r.bin").exists()
