@@ -252,6 +252,17 @@ def run_batch(args, rank, world, local_rank):
     sampler.__exit__()
     clocks = sampler.summary()
     complete = sum(1 for r in res if r.status == native.EMP_OK)
+    # finished instances against the CPU oracle's counts, where it could count them
+    verified = {"checked": 0, "mismatched": 0}
+    golden_path = os.path.join(ROOT, "tests", "golden", "batch_counts.json")
+    if os.path.exists(golden_path):
+        with open(golden_path) as f:
+            golden = {r["instance"]: (r["nodes"], r["solutions"]) for r in json.load(f)["records"]}
+        for j, r in enumerate(res):
+            idx = rank + world * j
+            if r.status == native.EMP_OK and idx in golden:
+                verified["checked"] += 1
+                verified["mismatched"] += int((r.nodes, r.solutions) != golden[idx])
     if args.counts_out and rank == 0:
         with open(args.counts_out, "w") as f:
             for j, (pz, r) in enumerate(zip(mine, res)):
@@ -299,6 +310,7 @@ def run_batch(args, rank, world, local_rank):
                                     "default_rate": tune.default_rate}},
             "gpu_launches": args.steps * (3 + 3 * max(rounds // max(args.steps, 1), 1)),
             "instances_complete": complete,
+            "instances_verified_on_rank0": verified,
             "roofline": {"bound": "hbm", "achieved": None, "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": None,
                          "traffic": None, "peak_source": peak_kind,
                          "note": "the DFS keeps its state on chip and reads tables through L1/L2 (66 MB of tables "

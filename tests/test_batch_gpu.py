@@ -135,3 +135,25 @@ def test_mixed_batch_sample_against_oracle():
             assert (r.nodes, r.solutions) == _oracle_counts(pz)
             checked += 1
     assert checked > 200
+
+
+def test_full_batch_against_cpu_counts():
+    """All 4096 instances of the batched workload in one graph launch with a deadline:
+    every instance the GPU finishes and the CPU oracle counted (tests/golden/
+    batch_counts.json, made by make_batch_counts.py) has exactly the oracle's counts, and
+    every instance the oracle counted quickly is finished."""
+    import json
+    import os
+    with open(os.path.join(os.path.dirname(__file__), "golden", "batch_counts.json")) as f:
+        golden = {r["instance"]: (r["nodes"], r["solutions"]) for r in json.load(f)["records"]}
+    batch = mixed_batch(4096)
+    handles = [native.NativePuzzle(p.width, p.height, p.colors) for p in batch]
+    res = native.bt_count_batch(handles, split_subtrees=1024, timeout_ms=4000, use_graph=1, table_placement=1)
+    checked = 0
+    for i, r in enumerate(res):
+        if r.status == native.EMP_OK and i in golden:
+            assert (r.nodes, r.solutions) == golden[i], i
+            checked += 1
+        if i in golden and golden[i][0] < 20000:
+            assert r.status == native.EMP_OK, i
+    assert checked >= 2000
