@@ -60,7 +60,7 @@ def main():
         for k, (i, side, nodes, sols, status, sec) in enumerate(pool.imap_unordered(_count, [j[1] for j in jobs])):
             if status == 0:
                 data["records"].append({"instance": i, "side": side, "nodes": nodes, "solutions": sols})
-            if k % 100 == 0 or k == len(jobs) - 1:
+            if k % 10 == 0 or k == len(jobs) - 1:
                 data["records"].sort(key=lambda r: r["instance"])
                 with open(OUT, "w") as f:
                     json.dump(data, f, indent=0)
