@@ -169,6 +169,48 @@ def board_string(width: int, height: int, cells: Sequence[int]) -> str:
     return "".join(out)
 
 
+def parse_board_string(width: int, height: int, text: str) -> List[int]:
+    """Inverse of board_string, as the reference reads a situation string
+    (include/situation_string_formatter.h:80-121): per row-major position a piece id on
+    digits(n) characters and an orientation letter, dashes for an empty cell.  Returns
+    (id-1)<<2|o per position, -1 when empty.  Raises ValueError on a malformed string
+    (the reference throws quicky_logic_exception)."""
+    n = width * height
+    wd = len(str(n)) + 1
+    if len(text) != n * wd:
+        raise ValueError(f"situation string of length {len(text)}, expected {n * wd}")
+    cells = []
+    for i in range(n):
+        cell = text[i * wd:(i + 1) * wd]
+        if cell[:-1] == "-" * (wd - 1):
+            cells.append(-1)
+            continue
+        if cell[-1] not in "NESW":
+            raise ValueError(f"bad orientation '{cell[-1]}' at position {i}")
+        pid = int(cell[:-1])
+        if not 1 <= pid <= n:
+            raise ValueError(f"bad piece id {pid} at position {i}")
+        cells.append(((pid - 1) << 2) | "NESW".index(cell[-1]))
+    return cells
+
+
+def situation_transitions(puzzle: "Puzzle", order: Sequence[int], cells: Sequence[int]) -> List[int]:
+    """Transitions t = kind_index << 2 | o of the situation's pieces along a position
+    order, up to the first empty position (include/emp_strategy.h:431-441)."""
+    kinds = [sum(1 for c in p if c == 0) for p in puzzle.colors]
+    kind_index, seen = [], [0, 0, 0]
+    for k in kinds:
+        kind_index.append(seen[k])
+        seen[k] += 1
+    out = []
+    for pos in order:
+        c = cells[pos]
+        if c < 0:
+            break
+        out.append((kind_index[c >> 2] << 2) | (c & 3))
+    return out
+
+
 def mixed_batch(count: int = 4096, seed: int = 2) -> List[Puzzle]:
     """The batched workload: ``count`` square puzzles whose side is drawn uniformly from
     4..9, border colours from 3..5 and interior colours from 4..10.  Instance i takes

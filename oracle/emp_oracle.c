@@ -463,8 +463,26 @@ static void dump_close(dumper *d, uint64_t total)
     free(d->words);
 }
 
+static int bt_run_impl(op_puzzle *p, const uint32_t *order, const uint16_t *situation, uint32_t placed,
+                       uint64_t node_limit, op_bt_result *out, const char *results_bin, char *maxlog,
+                       size_t maxlog_len);
+
 int op_bt_run(op_puzzle *p, const uint32_t *order, uint64_t node_limit, op_bt_result *out,
               const char *results_bin, char *maxlog, size_t maxlog_len)
+{
+    return bt_run_impl(p, order, NULL, 0, node_limit, out, results_bin, maxlog, maxlog_len);
+}
+
+int op_bt_resume(op_puzzle *p, const uint32_t *order, const uint16_t *situation, uint32_t placed,
+                 uint64_t node_limit, op_bt_result *out, const char *results_bin)
+{
+    if (!placed || placed >= p->n) return -1;
+    return bt_run_impl(p, order, situation, placed, node_limit, out, results_bin, NULL, 0);
+}
+
+static int bt_run_impl(op_puzzle *p, const uint32_t *order, const uint16_t *situation, uint32_t placed,
+                       uint64_t node_limit, op_bt_result *out, const char *results_bin, char *maxlog,
+                       size_t maxlog_len)
 {
     build_table(p);
     bt_state s;
@@ -480,6 +498,25 @@ int op_bt_run(op_puzzle *p, const uint32_t *order, uint64_t node_limit, op_bt_re
     uint32_t n = s.n, l_max = 0, idx = 0;
     uint64_t nodes = 0, sols = 0;
     int cont = 1;
+    if (placed) {
+        /* emp_strategy.h:418-467 (set_initial_state): each placed level takes its
+         * candidates in order up to the situation's transition, applying select_piece
+         * to every one tried; the search then starts at the LAST placed level (the
+         * loop steps back from the first empty position), whose candidate set
+         * specific_run recomputes from the start */
+        for (uint32_t l = 0; l < placed; ++l) {
+            bt_compute(&s, l);
+            uint32_t t;
+            do {
+                uint32_t t1 = bt_next(&s, l);
+                if (!t1) { free(board); bt_free(&s); dump_close(&d, 0); return -2; }
+                t = t1 - 1;
+                bt_select(&s, l, t);
+            } while (t != situation[l]);
+            s.piece_info[l] = p->binary[s.kind[l]][t];
+        }
+        idx = placed - 1;
+    }
     bt_compute(&s, idx);
     /* emp_strategy.h:343-410 */
     while (cont) {

@@ -83,6 +83,14 @@ int op_bt_run(op_puzzle *p, const uint32_t *order, uint64_t node_limit,
               op_bt_result *out, const char *results_bin,
               char *maxlog, size_t maxlog_len);
 
+/* The same search resumed from a partial situation, exactly
+ * emp_strategy::set_initial_state (include/emp_strategy.h:418-467) followed by
+ * specific_run: situation[l] is the transition placed at strategy level l for
+ * l < placed (0 < placed < n).  Returns -2 when a transition of the situation is
+ * not reachable in the reference's order, -1 on bad arguments. */
+int op_bt_resume(op_puzzle *p, const uint32_t *order, const uint16_t *situation, uint32_t placed,
+                 uint64_t node_limit, op_bt_result *out, const char *results_bin);
+
 /* Prefix expansion to depth d: enumerate every placement path of levels
  * 0..d-1 in the reference's visiting order.  prefixes receives up to
  * max_prefixes*d transitions.  Returns the number of prefixes at depth d;

@@ -78,6 +78,8 @@ def lib():
         L.op_table_entry.argtypes = [vp, u32, ctypes.POINTER(u64), u32]
         L.op_bt_run.argtypes = [vp, ctypes.POINTER(u32), u64, ctypes.POINTER(BtResult), ctypes.c_char_p,
                                 ctypes.c_char_p, ctypes.c_size_t]
+        L.op_bt_resume.argtypes = [vp, ctypes.POINTER(u32), ctypes.POINTER(ctypes.c_uint16), u32, u64,
+                                   ctypes.POINTER(BtResult), ctypes.c_char_p]
         L.op_bt_expand.restype = u64
         L.op_bt_expand.argtypes = [vp, ctypes.POINTER(u32), u32, ctypes.POINTER(ctypes.c_uint16), u64,
                                    ctypes.POINTER(u64), ctypes.POINTER(u64)]
@@ -153,6 +155,17 @@ class OraclePuzzle:
         lib().op_bt_run(self._p, self._order(order), node_limit, ctypes.byref(r),
                         results_bin.encode() if results_bin else None, log, cap)
         return r, (log.value.decode() if log is not None else "")
+
+    def resume(self, situation: Sequence[int], order=None, node_limit: int = 0, results_bin: Optional[str] = None):
+        """emp_strategy::set_initial_state + specific_run: ``situation`` holds the
+        transition placed at each of the first levels of the order."""
+        r = BtResult()
+        arr = (ctypes.c_uint16 * max(1, len(situation)))(*situation)
+        st = lib().op_bt_resume(self._p, self._order(order), arr, len(situation), node_limit, ctypes.byref(r),
+                                results_bin.encode() if results_bin else None)
+        if st:
+            raise ValueError(f"situation not reachable (status {st})")
+        return r
 
     def expand(self, depth: int, order=None, max_prefixes: int = 0):
         nn, ss = ctypes.c_uint64(), ctypes.c_uint64()
