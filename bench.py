@@ -521,6 +521,9 @@ def main():
     ap.add_argument("--full", action="store_true", help="run all slices (the complete count) and print per-seed totals")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
+    ap.add_argument("--host-loop", action="store_true",
+                    help="launch each DFS round from the host, one puzzle after another (the default runs each "
+                         "puzzle's rounds as one CUDA graph, puzzles on concurrent streams)")
     ap.add_argument("--workload", default="exhaustive", choices=["exhaustive", "batch", "glutton", "learned"],
                     help="exhaustive: the 16 seeded 8x8 puzzles (default); batch: 4096 mixed instances; "
                          "glutton: the 16x16 glutton max search; learned: time to a first solution, plain vs "
@@ -568,25 +571,42 @@ def main():
 
     from edge_matching_puzzle_b200 import native
     puzzles = make_puzzles()
-    # one plan per puzzle: each keeps its hot tables in shared memory
-    plans = [native.BtPlan([p], split_depth=DEPTH, device=local_rank) for p in puzzles]
+    # one plan per puzzle: each keeps its hot tables in shared memory.  By default each
+    # plan runs as one CUDA graph (every DFS round launched by the device) on a stream
+    # of its own, so the rounds of one puzzle fill the GPU while another drains.
+    graphs = not args.host_loop
+    plans = [native.BtPlan([p], split_depth=DEPTH, device=local_rank, use_graph=int(graphs)) for p in puzzles]
     counts = [pl.subtrees() for pl in plans]
     total_subtrees = sum(counts)
     flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.int32, device="cuda")
     start_ev = torch.cuda.Event(enable_timing=True)
     end_ev = torch.cuda.Event(enable_timing=True)
+    streams = [torch.cuda.Stream() for _ in plans] if graphs else []
 
     def slice_count(n, s):
         return (n - s + SLICES - 1) // SLICES if s < n else 0
 
     def run_slice(s):
-        """Runs slice s of every puzzle; returns the per-puzzle results."""
-        out = []
-        for pl, n in zip(plans, counts):
+        """Runs slice s of every puzzle; returns the per-puzzle results.  Graph runs:
+        the plans' graphs go out on their own streams (after start_ev) and end_ev waits
+        for all of them; host-loop runs: one plan after the other on the current stream."""
+        if not graphs:
+            out = []
+            for pl, n in zip(plans, counts):
+                pl.select(s, SLICES, slice_count(n, s))
+                pl.run()
+                out.append(pl.results()[0])
+            end_ev.record()
+            return out
+        cur = torch.cuda.current_stream()
+        for pl, n, st in zip(plans, counts, streams):
             pl.select(s, SLICES, slice_count(n, s))
-            pl.run()
-            out.append(pl.results()[0])
-        return out
+            st.wait_stream(cur)
+            pl.run(stream=st.cuda_stream)
+        for st in streams:
+            cur.wait_stream(st)
+        end_ev.record()
+        return [pl.results()[0] for pl in plans]
 
     if args.full:
         # the complete count of every workload puzzle (all subtrees, one run per puzzle)
@@ -625,8 +645,7 @@ def main():
         flush.add_(1)  # writes 252 MB: evicts L2 between steps
         barrier()
         start_ev.record()
-        res = run_slice(s)
-        end_ev.record()
+        res = run_slice(s)  # records end_ev
         barrier()
         if i >= args.warmup:
             t = start_ev.elapsed_time(end_ev)
@@ -636,7 +655,11 @@ def main():
             busy += sum(r.dfs_busy_ms for r in res)
             rounds += sum(r.rounds for r in res)
             records += sum(r.work_records + r.handed_back for r in res)
-            launches += sum(2 + r.rounds for r in res)  # make_records + reset + one DFS launch per round
+            if graphs:  # make_records, reset; per round a DFS launch, the round controller and (after the
+                # first) the record copy
+                launches += sum(2 + 3 * r.rounds - 1 for r in res)
+            else:  # make_records + reset + one DFS launch per round
+                launches += sum(2 + r.rounds for r in res)
     sampler.__exit__()
     clocks = sampler.summary()
     ms_max, (nodes_all,) = reduce_time_and_counts(dist, "cuda", ms, [float(nodes)])
@@ -684,7 +707,10 @@ def main():
         if kinds is None:
             kinds = [85, 14, 1]
         ops, byts, mix = algorithmic_work(kinds, puzzles[0])
-        launch_ms = busy / max(rounds, 1)
+        # host-loop runs time every DFS launch with events; graph runs (puzzles on concurrent
+        # streams, rounds launched by the device) give the timed region per launch, which
+        # also holds the small record-copy and round-controller kernels
+        launch_ms = (busy if not graphs else ms) / max(rounds, 1)
         placements_per_launch = nodes / max(rounds, 1)
         sm_clock = (clocks or {}).get("sm_max_mhz") or peaks.get("sm_max_mhz", 1965.0)
         rec_bytes = 4 * plans[0].rec_words()
@@ -718,7 +744,9 @@ def main():
             "clocks": clocks,
             "e2e": e2e,
             "cpu_baseline": cpu,
-            "dfs": {"rounds_per_step": rounds / args.steps, "busy_frac": busy / ms if ms else None},
+            "dfs": {"rounds_per_step": rounds / args.steps, "launch": "host loop" if not graphs else
+                    "one CUDA graph per puzzle slice (device-side round loop), 16 concurrent streams",
+                    "busy_frac": busy / ms if ms and not graphs else None},
         }
         oc = out["roofline_onchip"]
         oc["int_issue"]["frac"] = oc["int_issue"]["achieved_tops"] / oc["int_issue"]["peak_tops"]

@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstddef>
 #include <chrono>
 #include <cstring>
 #include <memory>
@@ -226,24 +227,40 @@ emp_status expand(emp_bt_plan_t& pl)
 
 }  // namespace
 
+// The records are built on the plan's own stream and a run waits for them on its
+// stream (ev_select), so a selection does not stall work queued on other streams.
+// Buffers only grow: the graph of a graph run stays valid while the initial-record
+// buffer stays where it is (its first round reads the record count on the device).
 emp_status plan_build_initial(emp_bt_plan_t& pl, uint64_t first, uint64_t stride, uint64_t count)
 {
-    CUDA_TRY(pl.rec_init.alloc(sizeof(uint32_t) * pl.rec_words * std::max<uint64_t>(count, 1)));
-    CUDA_TRY(emp::launch_make_records(pl.prefixes.as<uint16_t>(), pl.prefix_puzzle.as<uint32_t>(), pl.depth, first,
-                                      stride, count, pl.rec_words, pl.rec_init.as<uint32_t>(), nullptr,
-                                      pl.adaptive ? pl.puzzle_depth_dev.as<uint32_t>() : nullptr));
-    if (pl.cfg.keep_subtree_counts) {
-        CUDA_TRY(pl.item_nodes.alloc(sizeof(unsigned long long) * std::max<uint64_t>(count, 1)));
-        CUDA_TRY(pl.item_sols.alloc(sizeof(unsigned long long) * std::max<uint64_t>(count, 1)));
+    if (!pl.select_stream) {
+        CUDA_TRY(cudaStreamCreateWithFlags(&pl.select_stream, cudaStreamNonBlocking));
+        CUDA_TRY(cudaEventCreateWithFlags(&pl.ev_select, cudaEventDisableTiming));
     }
-    CUDA_TRY(cudaDeviceSynchronize());
+    // the previous run may still read the buffers: order the rebuild after it
+    if (pl.ran) CUDA_TRY(cudaStreamWaitEvent(pl.select_stream, pl.ev1, 0));
+    CUDA_TRY(pl.rec_init.reserve(sizeof(uint32_t) * pl.rec_words * std::max<uint64_t>(count, 1)));
+    if (pl.cfg.keep_subtree_counts) {
+        CUDA_TRY(pl.item_nodes.reserve(sizeof(unsigned long long) * std::max<uint64_t>(count, 1)));
+        CUDA_TRY(pl.item_sols.reserve(sizeof(unsigned long long) * std::max<uint64_t>(count, 1)));
+    }
+    CUDA_TRY(emp::launch_make_records(pl.prefixes.as<uint16_t>(), pl.prefix_puzzle.as<uint32_t>(), pl.depth, first,
+                                      stride, count, pl.rec_words, pl.rec_init.as<uint32_t>(), pl.select_stream,
+                                      pl.adaptive ? pl.puzzle_depth_dev.as<uint32_t>() : nullptr,
+                                      pl.ctl.as<emp::BtRunCtl>()));
+    CUDA_TRY(cudaEventRecord(pl.ev_select, pl.select_stream));
+    if (pl.graph_exec && pl.graph_rec_init != pl.rec_init.p) pl.drop_graph();
     pl.n_init = count;
     return EMP_OK;
 }
 
 namespace {
+struct ResumeSpec {
+    const uint16_t* situation;
+    uint32_t placed;
+};
 emp_status create_plan(const emp_puzzle* puzzles, uint32_t count, const emp_bt_config* config, bool dump,
-                       emp_bt_plan* out);
+                       emp_bt_plan* out, const ResumeSpec* resume = nullptr);
 }  // namespace
 
 extern "C" emp_status emp_bt_plan_create(const emp_puzzle* puzzles, uint32_t count, const emp_bt_config* config,
@@ -254,8 +271,86 @@ extern "C" emp_status emp_bt_plan_create(const emp_puzzle* puzzles, uint32_t cou
 
 namespace {
 
+// Work records of a search resumed from a partial situation: what
+// emp_strategy::set_initial_state leaves for specific_run
+// (include/emp_strategy.h:418-467).  Each placed level takes its candidates in
+// order up to the situation's transition, applying select_piece (and so the
+// identical-piece masks) to every one tried; the search then starts at the LAST
+// placed level (the loop steps back from the first empty position), whose
+// candidate set specific_run recomputes in full, and it ends when level 1 is
+// exhausted (:398, level 0 keeps its transition).  So the records, in visiting
+// order, are: the last placed level with all its candidates, then every shallower
+// level down to level 1 with the candidates it has left.  The candidate words come
+// from the same tables the kernels read.
+emp_status resume_records(const emp_puzzle_t& pz, const uint16_t* situation, uint32_t placed, uint32_t rec_words,
+                          uint32_t max_kw, std::vector<uint32_t>& recs, uint64_t& count)
+{
+    const std::vector<uint32_t>& b = pz.tables.blob;
+    const uint32_t n = b[1], ncol = b[2], desc_off = b[14], init = b[21], aw = b[9];
+    if (placed < 2 || placed >= n)
+        return fail(EMP_ERR_INVALID, "emp_bt_resume: the situation must place between 2 and n-1 pieces");
+    std::vector<uint32_t> av(b.begin() + init, b.begin() + init + aw), stk(n, 0);
+    std::vector<std::vector<uint32_t>> rem(placed);
+    std::vector<uint8_t> spilled(placed, 0);
+    auto facing = [&](uint32_t e, uint32_t side) { return (e >> (5 * ((side + 2) & 3u))) & 31u; };
+    for (uint32_t l = 0; l < placed; ++l) {
+        const uint32_t* d = &b[desc_off + 8 * l];
+        const uint32_t kw = d[0] & 0xFFu, nextra = (d[0] >> 13) & 7u, aoff = d[0] >> 16;
+        const uint32_t ea = stk[d[1] & 0xFFu], eb = stk[(d[1] >> 8) & 0xFFu];
+        const uint32_t row = d[2] + ((ea >> ((d[1] >> 16) & 0xFFu)) & 31u) * (d[3] & 0xFFFFu) +
+                             ((eb >> (d[1] >> 24)) & 31u) * (d[3] >> 16);
+        std::vector<uint32_t> c(kw);
+        for (uint32_t w = 0; w < kw; ++w) c[w] = b[row + 1 + w] & av[aoff + w];
+        for (uint32_t j = 0; j < nextra; ++j) {
+            const uint32_t sd = (d[7] >> (2 * j)) & 3u, lev = (d[7] >> (8 + 8 * j)) & 0xFFu;
+            const uint32_t* sm = &b[d[4] + (sd * ncol + facing(stk[lev], sd)) * kw];
+            for (uint32_t w = 0; w < kw; ++w) c[w] &= sm[w];
+        }
+        const uint32_t want = situation[l];
+        uint32_t t = ~0u;
+        while (t != want) {
+            t = ~0u;
+            for (uint32_t w = 0; w < kw && t == ~0u; ++w)
+                if (c[w]) t = 32 * w + static_cast<uint32_t>(__builtin_ctz(c[w]));
+            if (t == ~0u)
+                return fail(EMP_ERR_INVALID, "emp_bt_resume: the situation's piece at level " + std::to_string(l) +
+                                                 " is not reachable in the search order");
+            const uint32_t ti = b[d[5] + t];
+            if ((ti >> 20) & 1u) {  // select_piece with an identical mask (emp_position_strategy.h:197-200)
+                for (uint32_t w = 0; w < kw; ++w) c[w] &= b[d[6] + t * kw + w];
+                spilled[l] = 1;
+            } else {
+                c[t >> 5] &= ~(1u << (t & 31u));
+            }
+        }
+        rem[l] = c;
+        av[aoff + (t >> 5)] &= ~(0xFu << (t & 28u));
+        stk[l] = b[d[5] + t] & 0xFFFFFu;
+    }
+    recs.clear();
+    count = 0;
+    auto emit = [&](uint32_t len, uint32_t start, const std::vector<uint32_t>* rest) {
+        std::vector<uint32_t> r(rec_words, 0);
+        r[0] = static_cast<uint32_t>(count);
+        r[2] = len | (start << 16);
+        r[3] = rest ? (1u << 16) : 0u;
+        for (uint32_t j = 0; j < len; ++j) r[4 + (j >> 1)] |= static_cast<uint32_t>(situation[j]) << (16 * (j & 1));
+        if (rest)
+            for (uint32_t w = 0; w < rest->size() && w < max_kw; ++w) r[rec_words - max_kw + w] = (*rest)[w];
+        recs.insert(recs.end(), r.begin(), r.end());
+        ++count;
+    };
+    emit(placed - 1, 0, nullptr);
+    for (uint32_t l = placed - 1; l-- > 1;) {
+        bool any = false;
+        for (uint32_t v : rem[l]) any = any || v;
+        if (any) emit(l, situation[l] + 1u, spilled[l] ? &rem[l] : nullptr);
+    }
+    return EMP_OK;
+}
+
 emp_status create_plan(const emp_puzzle* puzzles, uint32_t count, const emp_bt_config* config, bool dump,
-                       emp_bt_plan* out)
+                       emp_bt_plan* out, const ResumeSpec* resume)
 {
     emp::clear_error();
     if (!puzzles || !count || !out) return fail(EMP_ERR_INVALID, "emp_bt_plan_create: no puzzle");
@@ -275,9 +370,11 @@ emp_status create_plan(const emp_puzzle* puzzles, uint32_t count, const emp_bt_c
         pl->max_avail = std::max(pl->max_avail, t.avail_words);
         pl->max_kw = std::max(pl->max_kw, t.max_kw);
     }
-    pl->adaptive = pl->cfg.split_subtrees != 0;
-    pl->depth = pl->cfg.split_depth ? pl->cfg.split_depth : auto_depth(min_n);
-    if (pl->adaptive) {
+    pl->adaptive = pl->cfg.split_subtrees != 0 && !resume;
+    pl->depth = resume ? 0u : (pl->cfg.split_depth ? pl->cfg.split_depth : auto_depth(min_n));
+    if (resume) {
+        if (count != 1) return fail(EMP_ERR_INVALID, "emp_bt_resume: one puzzle");
+    } else if (pl->adaptive) {
         if (pl->cfg.split_depth > 64)
             return fail(EMP_ERR_INVALID, "emp_bt_plan_create: split depth limit must be at most 64");
     } else if (pl->depth >= min_n || pl->depth > 64) {
@@ -310,7 +407,16 @@ emp_status create_plan(const emp_puzzle* puzzles, uint32_t count, const emp_bt_c
     CUDA_TRY(cudaEventCreate(&pl->evr1));
     if (pl->cfg.use_graph) CUDA_TRY(cudaStreamCreateWithFlags(&pl->capture_stream, cudaStreamNonBlocking));
     pl->dump = dump;
-    EMP_TRY(expand(*pl));
+    std::vector<uint32_t> resume_recs;
+    if (resume) {
+        EMP_TRY(resume_records(*pl->puzzles[0], resume->situation, resume->placed, pl->rec_words, pl->max_kw,
+                               resume_recs, pl->n_all));
+        pl->exp_nodes.assign(1, 0);
+        pl->exp_sols.assign(1, 0);
+        pl->puzzle_depth.assign(1, 0);
+    } else {
+        EMP_TRY(expand(*pl));
+    }
     // hot tables in shared memory when the plan holds one puzzle
     const uint32_t hot = (pl->puzzles[0]->tables.blob[26] + 3u) & ~3u;
     const bool want_smem = pl->cfg.table_placement == 2 || (pl->cfg.table_placement == 0 && count == 1);
@@ -320,14 +426,14 @@ emp_status create_plan(const emp_puzzle* puzzles, uint32_t count, const emp_bt_c
     // launch geometry: the block size with the most resident warps per SM
     cudaDeviceProp prop;
     CUDA_TRY(cudaGetDeviceProperties(&prop, pl->device));
-    if (pl->max_kw > 16) return fail(EMP_ERR_UNSUPPORTED, "puzzle kinds wider than 16 64-bit words");
+    if (pl->max_kw > 32) return fail(EMP_ERR_UNSUPPORTED, "puzzle kinds wider than 32 candidate words");
     std::vector<uint32_t> candidates;
     if (pl->cfg.threads_per_block) candidates.push_back(pl->cfg.threads_per_block);
-    else candidates = {64, 128, 256};
+    else candidates = {64, 128, 256, 512};
     int best_warps = 0;
     for (uint32_t threads : candidates) {
         const void* fn = emp::dfs_kernel_symbol(pl->max_kw, pl->smem_tab_words != 0, threads);
-        if (!fn) return fail(EMP_ERR_INVALID, "threads_per_block must be 64, 128 or 256");
+        if (!fn) return fail(EMP_ERR_INVALID, "threads_per_block must be 64, 128, 256 or 512");
         const size_t smem = emp::dfs_smem_bytes(pl->max_levels, pl->max_avail, threads, pl->smem_tab_words);
         if (smem > static_cast<size_t>(prop.sharedMemPerBlockOptin)) continue;
         CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
@@ -343,7 +449,7 @@ emp_status create_plan(const emp_puzzle* puzzles, uint32_t count, const emp_bt_c
     }
     if (!best_warps)
         return fail(EMP_ERR_UNSUPPORTED, "per-thread DFS state does not fit shared memory; use fewer threads per block");
-    CUDA_TRY(pl->spill.alloc(sizeof(uint64_t) * static_cast<size_t>(pl->blocks) * pl->threads * pl->max_levels *
+    CUDA_TRY(pl->spill.alloc(sizeof(uint32_t) * static_cast<size_t>(pl->blocks) * pl->threads * pl->max_levels *
                              pl->max_kw));
     // round queues: room for every resident thread to hand back a full path twice
     const uint64_t resident = static_cast<uint64_t>(pl->blocks) * pl->threads;
@@ -352,7 +458,22 @@ emp_status create_plan(const emp_puzzle* puzzles, uint32_t count, const emp_bt_c
     CUDA_TRY(pl->rec_a.alloc(sizeof(uint32_t) * pl->rec_words * pl->capacity));
     CUDA_TRY(pl->rec_b.alloc(sizeof(uint32_t) * pl->rec_words * pl->capacity));
     pl->budget = pl->cfg.split_budget ? pl->cfg.split_budget : 2048u;
-    EMP_TRY(plan_build_initial(*pl, 0, 1, pl->n_all));
+    if (resume) {
+        CUDA_TRY(pl->rec_init.reserve(sizeof(uint32_t) * resume_recs.size()));
+        CUDA_TRY(cudaMemcpy(pl->rec_init.p, resume_recs.data(), sizeof(uint32_t) * resume_recs.size(),
+                            cudaMemcpyHostToDevice));
+        const unsigned long long n_init = pl->n_all;
+        CUDA_TRY(cudaMemcpy(reinterpret_cast<char*>(pl->ctl.p) + offsetof(emp::BtRunCtl, n_init), &n_init,
+                            sizeof(n_init), cudaMemcpyHostToDevice));
+        if (pl->cfg.keep_subtree_counts) {
+            CUDA_TRY(pl->item_nodes.reserve(sizeof(unsigned long long) * pl->n_all));
+            CUDA_TRY(pl->item_sols.reserve(sizeof(unsigned long long) * pl->n_all));
+        }
+        pl->n_init = pl->n_all;
+        pl->resumed = true;
+    } else {
+        EMP_TRY(plan_build_initial(*pl, 0, 1, pl->n_all));
+    }
     *out = pl.release();
     return EMP_OK;
 }
@@ -371,10 +492,10 @@ extern "C" emp_status emp_bt_plan_select(emp_bt_plan plan, uint64_t first, uint6
 {
     emp::clear_error();
     if (!plan || !stride) return fail(EMP_ERR_INVALID, "emp_bt_plan_select: null plan or zero stride");
+    if (plan->resumed) return fail(EMP_ERR_INVALID, "emp_bt_plan_select: not for a resumed search");
     if (count && first + (count - 1) * stride >= plan->n_all)
         return fail(EMP_ERR_INVALID, "emp_bt_plan_select: selection past the last subtree");
     CUDA_TRY(cudaSetDevice(plan->device));
-    plan->drop_graph();  // the graph holds the previous selection's records
     EMP_TRY(plan_build_initial(*plan, first, stride, count));
     plan->sampled = true;
     return EMP_OK;
@@ -399,8 +520,10 @@ emp_status build_graph(emp_bt_plan_t& pl)
     CUDA_TRY(cudaGraphConditionalHandleCreate(&loop, g, 0, 0));
     emp::BtLaunch P = pl.launch();
     P.in_rec = pl.rec_init.as<uint32_t>();
-    P.n_in = pl.n_init;
+    P.n_in = 0;
+    P.n_in_from_ctl = 1;  // the selection's count, left in the run control block by make_records
     P.out_rec = pl.rec_b.as<uint32_t>();
+    pl.graph_rec_init = pl.rec_init.p;
     CUDA_TRY(cudaStreamBeginCaptureToGraph(cs, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
     cudaError_t e = emp::launch_bt_reset(P, static_cast<uint32_t>(pl.puzzles.size()), cs);
     if (e == cudaSuccess) e = cudaMemsetAsync(pl.counters.p, 0, pl.counters.bytes, cs);
@@ -433,8 +556,6 @@ emp_status build_graph(emp_bt_plan_t& pl)
     cudaGraph_t body = cp.conditional.phGraph_out[0];
     emp::BtLaunch Q = P;
     Q.in_rec = pl.rec_a.as<uint32_t>();
-    Q.n_in = 0;
-    Q.n_in_from_ctl = 1;
     CUDA_TRY(cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
     e = emp::launch_round_copy(Q, pl.rec_a.as<uint32_t>(), pl.rec_b.as<uint32_t>(), cs);
     if (e == cudaSuccess) e = emp::launch_dfs(Q, pl.blocks, pl.threads, cs);
@@ -454,6 +575,7 @@ extern "C" emp_status emp_bt_plan_run(emp_bt_plan plan, void* stream)
     if (!plan) return fail(EMP_ERR_INVALID, "emp_bt_plan_run: null plan");
     CUDA_TRY(cudaSetDevice(plan->device));
     cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (plan->ev_select) CUDA_TRY(cudaStreamWaitEvent(st, plan->ev_select, 0));
     if (plan->cfg.use_graph) {
         if (!plan->graph_exec) {
             const emp_status s = build_graph(*plan);
@@ -555,7 +677,7 @@ extern "C" emp_status emp_bt_plan_results(emp_bt_plan plan, emp_bt_result* resul
         r.expansion_nodes = plan->exp_nodes[i];
         r.nodes = tot[2 * i] + (plan->sampled ? 0 : plan->exp_nodes[i]);
         r.solutions = tot[2 * i + 1] + (plan->sampled ? 0 : plan->exp_sols[i]);
-        r.status = incomplete[i] ? EMP_INCOMPLETE : EMP_OK;
+        r.status = incomplete[i] ? EMP_INCOMPLETE : (rec[i].missed ? EMP_FIRST_LOST : EMP_OK);
         r.kernel_ms = ms;
         r.rounds = plan->rounds;
         r.first_found_us = first_found_us;
@@ -596,6 +718,7 @@ extern "C" emp_status emp_bt_plan_subtree_prefix(emp_bt_plan plan, uint64_t inde
     if (!plan || !prefix) return fail(EMP_ERR_INVALID, "emp_bt_plan_subtree_prefix: null argument");
     if (index >= plan->n_init || capacity < plan->depth) return fail(EMP_ERR_INVALID, "emp_bt_plan_subtree_prefix: bad index");
     CUDA_TRY(cudaSetDevice(plan->device));
+    if (plan->ev_select) CUDA_TRY(cudaEventSynchronize(plan->ev_select));
     CUDA_TRY(emp::launch_record_prefix(plan->rec_init.as<uint32_t>(), plan->rec_words, index,
                                        plan->prefix_out.as<uint16_t>(), nullptr));
     CUDA_TRY(cudaMemcpy(prefix, plan->prefix_out.p, sizeof(uint16_t) * plan->depth, cudaMemcpyDeviceToHost));
@@ -650,12 +773,15 @@ extern "C" emp_status emp_bt_count_batch(const emp_puzzle* puzzles, uint32_t cou
     }
     if (s != EMP_OK) return s;
     const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
-    bool incomplete = false;
+    bool incomplete = false, lost = false;
     for (uint32_t i = 0; i < count; ++i) {
         results[i].total_ms = ms;
         incomplete |= results[i].status == EMP_INCOMPLETE;
+        lost |= results[i].status == EMP_FIRST_LOST;
     }
-    return incomplete ? EMP_INCOMPLETE : EMP_OK;
+    if (incomplete) return EMP_INCOMPLETE;
+    if (lost) return fail(EMP_FIRST_LOST, "a first-solution record was not written: its lock wait ran out");
+    return EMP_OK;
 }
 
 extern "C" emp_status emp_bt_count(emp_puzzle puzzle, const emp_bt_config* config, emp_bt_result* result)
@@ -663,8 +789,36 @@ extern "C" emp_status emp_bt_count(emp_puzzle puzzle, const emp_bt_config* confi
     return emp_bt_count_batch(&puzzle, 1, config, result);
 }
 
-extern "C" emp_status emp_bt_solutions(emp_puzzle puzzle, const emp_bt_config* config, emp_bt_solution* out,
-                                       uint64_t capacity, uint64_t* found, emp_bt_result* result)
+extern "C" emp_status emp_bt_resume(emp_puzzle puzzle, const uint16_t* situation, uint32_t placed,
+                                    const emp_bt_config* config, emp_bt_result* result)
+{
+    emp::clear_error();
+    if (!puzzle || !result || (placed && !situation)) return fail(EMP_ERR_INVALID, "emp_bt_resume: null argument");
+    if (placed <= 1) return emp_bt_count(puzzle, config, result);  // the search starts at level 0 as usual
+    emp_bt_config cfg{};
+    cfg.device = -1;
+    if (config) cfg = *config;
+    cfg.sample_stride = 0;
+    cfg.split_subtrees = 0;
+    const ResumeSpec spec{situation, placed};
+    emp_bt_plan plan = nullptr;
+    emp_status s = create_plan(&puzzle, 1, &cfg, false, &plan, &spec);
+    if (s != EMP_OK) return s;
+    std::unique_ptr<emp_bt_plan_t> guard(plan);
+    s = emp_bt_plan_run(plan, nullptr);
+    if (s != EMP_OK) return s;
+    s = emp_bt_plan_results(plan, result);
+    if (s != EMP_OK) return s;
+    if (result->status == EMP_INCOMPLETE) return EMP_INCOMPLETE;
+    if (result->status == EMP_FIRST_LOST)
+        return fail(EMP_FIRST_LOST, "a first-solution record was not written: its lock wait ran out");
+    return EMP_OK;
+}
+
+namespace {
+
+emp_status solutions_impl(emp_puzzle puzzle, const emp_bt_config* config, const ResumeSpec* resume,
+                          emp_bt_solution* out, uint64_t capacity, uint64_t* found, emp_bt_result* result)
 {
     emp::clear_error();
     if (!puzzle || !found || (capacity && !out)) return fail(EMP_ERR_INVALID, "emp_bt_solutions: null argument");
@@ -678,25 +832,38 @@ extern "C" emp_status emp_bt_solutions(emp_puzzle puzzle, const emp_bt_config* c
     cfg.use_graph = 0;
     cfg.split_subtrees = 0;
     emp_bt_plan plan = nullptr;
-    emp_status s = create_plan(&puzzle, 1, &cfg, true, &plan);
+    emp_status s = create_plan(&puzzle, 1, &cfg, true, &plan, resume);
     if (s != EMP_OK) return s;
     std::unique_ptr<emp_bt_plan_t> guard(plan);
     plan->budget = 0;  // never hand work back: each subtree is searched in order by one thread
-    const uint64_t cap = std::max<uint64_t>(capacity, 1);
-    CUDA_TRY(plan->sol_buf.alloc(sizeof(emp::SolutionRecord) * cap));
     CUDA_TRY(plan->sol_count.alloc(sizeof(unsigned long long)));
-    CUDA_TRY(cudaMemset(plan->sol_count.p, 0, sizeof(unsigned long long)));
-    plan->sol_capacity = capacity;
-    s = emp_bt_plan_run(plan, nullptr);
-    if (s != EMP_OK) return s;
+    // Threads record solutions in arrival order; ranking them needs all of them.  When
+    // more solutions exist than the caller holds, the (deterministic) search runs
+    // again with room for every one, and the first `capacity` by node index are kept.
+    constexpr uint64_t kMaxRanked = 1ull << 20;
+    uint64_t room = std::max<uint64_t>(capacity, 1);
     emp_bt_result res{};
-    s = emp_bt_plan_results(plan, &res);
-    if (s != EMP_OK) return s;
-    if (result) *result = res;
-    if (res.status != EMP_OK) return fail(EMP_INCOMPLETE, "emp_bt_solutions: the search stopped before the end");
     unsigned long long total = 0;
-    CUDA_TRY(cudaMemcpy(&total, plan->sol_count.p, sizeof(total), cudaMemcpyDeviceToHost));
+    for (int pass = 0; pass < 2; ++pass) {
+        CUDA_TRY(plan->sol_buf.alloc(sizeof(emp::SolutionRecord) * room));
+        CUDA_TRY(cudaMemset(plan->sol_count.p, 0, sizeof(unsigned long long)));
+        plan->sol_capacity = room;
+        s = emp_bt_plan_run(plan, nullptr);
+        if (s != EMP_OK) return s;
+        s = emp_bt_plan_results(plan, &res);
+        if (s != EMP_OK) return s;
+        if (result) *result = res;
+        if (res.status == EMP_INCOMPLETE)
+            return fail(EMP_INCOMPLETE, "emp_bt_solutions: the search stopped before the end");
+        CUDA_TRY(cudaMemcpy(&total, plan->sol_count.p, sizeof(total), cudaMemcpyDeviceToHost));
+        if (total <= room) break;
+        if (total > kMaxRanked)
+            return fail(EMP_ERR_UNSUPPORTED, "emp_bt_solutions: more than 2^20 solutions to rank; count them with "
+                                             "emp_bt_count and dump them with a capacity of at least the count");
+        room = total;
+    }
     *found = total;
+    const uint64_t nall = std::min<uint64_t>(total, room);  // every solution when a second pass ran
     const uint64_t nsol = std::min<uint64_t>(total, capacity);
     if (!nsol) return EMP_OK;
     // level arrays: device pointer table (index L = prefixes of length L)
@@ -710,19 +877,19 @@ extern "C" emp_status emp_bt_solutions(emp_puzzle puzzle, const emp_bt_config* c
     DeviceBuffer d_ptrs, d_counts, d_idx;
     CUDA_TRY(d_ptrs.alloc(sizeof(void*) * ptrs.size()));
     CUDA_TRY(d_counts.alloc(sizeof(uint64_t) * counts.size()));
-    CUDA_TRY(d_idx.alloc(sizeof(unsigned long long) * nsol));
+    CUDA_TRY(d_idx.alloc(sizeof(unsigned long long) * nall));
     CUDA_TRY(cudaMemcpy(d_ptrs.p, ptrs.data(), sizeof(void*) * ptrs.size(), cudaMemcpyHostToDevice));
     CUDA_TRY(cudaMemcpy(d_counts.p, counts.data(), sizeof(uint64_t) * counts.size(), cudaMemcpyHostToDevice));
-    CUDA_TRY(emp::launch_solution_index(plan->sol_buf.as<emp::SolutionRecord>(), nsol,
+    CUDA_TRY(emp::launch_solution_index(plan->sol_buf.as<emp::SolutionRecord>(), nall,
                                         reinterpret_cast<const uint16_t* const*>(d_ptrs.p), d_counts.as<uint64_t>(),
                                         depth, plan->item_nodes.as<unsigned long long>(),
                                         d_idx.as<unsigned long long>(), nullptr));
-    std::vector<emp::SolutionRecord> recs(nsol);
-    std::vector<unsigned long long> idx(nsol);
-    CUDA_TRY(cudaMemcpy(recs.data(), plan->sol_buf.p, sizeof(emp::SolutionRecord) * nsol, cudaMemcpyDeviceToHost));
-    CUDA_TRY(cudaMemcpy(idx.data(), d_idx.p, sizeof(unsigned long long) * nsol, cudaMemcpyDeviceToHost));
-    std::vector<uint64_t> order(nsol);
-    for (uint64_t i = 0; i < nsol; ++i) order[i] = i;
+    std::vector<emp::SolutionRecord> recs(nall);
+    std::vector<unsigned long long> idx(nall);
+    CUDA_TRY(cudaMemcpy(recs.data(), plan->sol_buf.p, sizeof(emp::SolutionRecord) * nall, cudaMemcpyDeviceToHost));
+    CUDA_TRY(cudaMemcpy(idx.data(), d_idx.p, sizeof(unsigned long long) * nall, cudaMemcpyDeviceToHost));
+    std::vector<uint64_t> order(nall);
+    for (uint64_t i = 0; i < nall; ++i) order[i] = i;
     std::sort(order.begin(), order.end(), [&](uint64_t a, uint64_t b) { return idx[a] < idx[b]; });
     const emp::PuzzleModel& m = puzzle->model;
     for (uint64_t k = 0; k < nsol; ++k) {
@@ -737,4 +904,22 @@ extern "C" emp_status emp_bt_solutions(emp_puzzle puzzle, const emp_bt_config* c
         }
     }
     return EMP_OK;
+}
+
+}  // namespace
+
+extern "C" emp_status emp_bt_solutions(emp_puzzle puzzle, const emp_bt_config* config, emp_bt_solution* out,
+                                       uint64_t capacity, uint64_t* found, emp_bt_result* result)
+{
+    return solutions_impl(puzzle, config, nullptr, out, capacity, found, result);
+}
+
+extern "C" emp_status emp_bt_resume_solutions(emp_puzzle puzzle, const uint16_t* situation, uint32_t placed,
+                                              const emp_bt_config* config, emp_bt_solution* out, uint64_t capacity,
+                                              uint64_t* found, emp_bt_result* result)
+{
+    if (placed <= 1) return solutions_impl(puzzle, config, nullptr, out, capacity, found, result);
+    if (!situation) return fail(EMP_ERR_INVALID, "emp_bt_resume_solutions: null situation");
+    const ResumeSpec spec{situation, placed};
+    return solutions_impl(puzzle, config, &spec, out, capacity, found, result);
 }

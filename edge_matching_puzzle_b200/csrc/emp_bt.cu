@@ -13,8 +13,11 @@
 //
 // Per-thread DFS state lives in shared memory, thread-interleaved so that a
 // warp touching "its" entries hits 32 distinct banks:
-//   stk[L*T + tid]  = t << 21 | spilled << 20 | colours of the placed piece
-//   av[w*T + tid]   = availability words of all three kinds
+//   stk[L*T + tid]  = more << 31 | t << 21 | spilled << 20 | colours of the placed piece
+//   av[w*T + tid]   = 32-bit availability words of all three kinds
+// Candidate sets are 32-bit words (8 pieces x 4 orientations each).  A level's
+// pair-table row starts with an occupancy word (bit w: candidate word w is not
+// zero), so a try reads only the words that can hold a candidate.
 // The identical-piece case needs the exact remaining-candidate set of a level
 // once a transition with a non-trivial mask has been tried there; such a level
 // keeps its set in a per-thread global scratch row (spill) until it is left.
@@ -34,14 +37,22 @@ namespace {
 
 constexpr unsigned kFull = 0xFFFFFFFFu;
 constexpr uint32_t kMaxExpandDepth = 64;
-constexpr uint32_t kMaxAvailWords = 24;   // 64-bit availability words, three kinds
-constexpr uint32_t kMaxKindWords = 16;    // 64-bit words of one kind (256 pieces)
+constexpr uint32_t kMaxAvailWords = 40;   // 32-bit availability words, three kinds (256 pieces)
+constexpr uint32_t kMaxKindWords = 32;    // 32-bit words of one kind (256 pieces x 4 orientations)
 
 __device__ __forceinline__ uint64_t global_ns()
 {
     uint64_t t;
     asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
     return t;
+}
+
+// 32-bit shift left whose amount saturates at 32 (PTX clamps shift amounts)
+__device__ __forceinline__ uint32_t shl32(uint32_t v, uint32_t n)
+{
+    uint32_t r;
+    asm("shl.b32 %0, %1, %2;" : "=r"(r) : "r"(v), "r"(n));
+    return r;
 }
 
 // ---------------------------------------------------------------------------
@@ -72,15 +83,15 @@ __global__ void expand_kernel(BtLaunch P, const uint16_t* __restrict__ parents,
         }
         const uint32_t* tb = P.tables + P.puzzle_offset[pz];
         const uint32_t n = ldg(tb + H_N), ncol = ldg(tb + H_NCOL), desc_off = ldg(tb + H_DESC);
-        uint64_t av[kMaxAvailWords];
+        uint32_t av[kMaxAvailWords];
         uint32_t stk[kMaxExpandDepth];
         const uint32_t aw = ldg(tb + H_AWORDS), init = ldg(tb + H_INIT);
-        for (uint32_t w = 0; w < aw; ++w) av[w] = ldg64(tb + init + 2 * w);
+        for (uint32_t w = 0; w < aw; ++w) av[w] = ldg(tb + init + w);
         const uint16_t* pre = parents + i * level;
         for (uint32_t l = 0; l < level; ++l) {
             const LevelDesc d = load_desc(tb, desc_off, l);
             const uint32_t t = pre[l];
-            av[d.aoff() + (t >> 6)] &= ~(0xFull << (t & 60u));
+            av[d.aoff() + (t >> 5)] &= ~(0xFu << (t & 28u));
             stk[l] = ldg(tb + d.d5 + t) & 0xFFFFFu;
         }
         uint32_t cnt = 0;
@@ -88,18 +99,18 @@ __global__ void expand_kernel(BtLaunch P, const uint16_t* __restrict__ parents,
             const LevelDesc d = load_desc(tb, desc_off, level);
             const uint32_t kw = d.kw();
             const uint32_t row = d.row(stk[d.level_a()], stk[d.level_b()]);
-            uint64_t R[kMaxKindWords];
-            for (uint32_t w = 0; w < kw; ++w) R[w] = ldg64(tb + row + 2 * w) & av[d.aoff() + w];
+            uint32_t R[kMaxKindWords];
+            for (uint32_t w = 0; w < kw; ++w) R[w] = ldg(tb + row + 1 + w) & av[d.aoff() + w];
             for (uint32_t j = 0; j < d.nextra(); ++j) {
                 const uint32_t sd = d.extra_side(j);
                 const uint32_t c = facing_colour(stk[d.extra_level(j)], sd);
-                const uint32_t* sm = tb + d.d4 + ((sd * ncol + c) * kw) * 2;
-                for (uint32_t w = 0; w < kw; ++w) R[w] &= ldg64(sm + 2 * w);
+                const uint32_t* sm = tb + d.d4 + (sd * ncol + c) * kw;
+                for (uint32_t w = 0; w < kw; ++w) R[w] &= ldg(sm + w);
             }
             uint64_t out = mode ? offsets[i] : 0;
             for (uint32_t w = 0; w < kw; ++w) {
                 while (R[w]) {
-                    const uint32_t t = w * 64 + __ffsll(R[w]) - 1;
+                    const uint32_t t = w * 32 + __ffs(R[w]) - 1;
                     if (mode) {
                         uint16_t* c = children + out * (level + 1);
                         for (uint32_t l = 0; l < level; ++l) c[l] = pre[l];
@@ -113,10 +124,10 @@ __global__ void expand_kernel(BtLaunch P, const uint16_t* __restrict__ parents,
                         break;
                     }
                     if ((ldg(tb + d.d5 + t) >> 20) & 1u) {
-                        const uint32_t* ex = tb + d.d6 + t * kw * 2;
-                        for (uint32_t ww = 0; ww < kw; ++ww) R[ww] &= ldg64(ex + 2 * ww);
+                        const uint32_t* ex = tb + d.d6 + t * kw;
+                        for (uint32_t ww = 0; ww < kw; ++ww) R[ww] &= ldg(ex + ww);
                     } else {
-                        R[w] &= ~(1ull << (t & 63));
+                        R[w] &= ~(1u << (t & 31));
                     }
                 }
             }
@@ -209,14 +220,15 @@ __global__ void scan_apply(const uint32_t* __restrict__ in, uint64_t n, const ui
 //
 // record words: [0,1] subtree id (for per-subtree counts), [2] len | start<<16,
 // [3] puzzle | spilled<<16 | empty<<17, [4..] transitions (u16 pairs), then
-// the remaining set of level len (max_kw 64-bit words as u32 pairs).
+// the remaining set of level len (max_kw 32-bit words).
 //
 // Per-thread state in shared memory, thread-interleaved with a compile-time
 // block size T (a warp touching its own entries hits distinct banks and every
 // address is base + immediate):
 //   stk[L*T + tid] = more<<31 | t<<21 | spilled<<20 | colours of the placed piece
-//                    (more: candidates remained after t when it was placed)
-//   av[w*T + tid]  = 64-bit availability words of the three kinds
+//                    (more: candidates may remain after t; exact within t's word,
+//                    over-approximated by the row's occupancy beyond it)
+//   av[w*T + tid]  = 32-bit availability words of the three kinds
 struct ThreadItem {
     uint64_t orig;
     const uint32_t* tb;
@@ -238,10 +250,6 @@ struct Tab;
 template <>
 struct Tab<true> {
     static __device__ __forceinline__ uint32_t u32(const ThreadItem&, uint32_t off) { return g_smem[off]; }
-    static __device__ __forceinline__ uint64_t u64(const ThreadItem&, uint32_t off)
-    {
-        return reinterpret_cast<const unsigned long long*>(g_smem)[off >> 1];
-    }
     static __device__ __forceinline__ LevelDesc desc(const ThreadItem& s, uint32_t L)
     {
         const uint4* d = reinterpret_cast<const uint4*>(g_smem + s.desc_off + 8 * L);
@@ -253,20 +261,11 @@ struct Tab<true> {
 template <>
 struct Tab<false> {
     static __device__ __forceinline__ uint32_t u32(const ThreadItem& s, uint32_t off) { return ldg(s.tb + off); }
-    static __device__ __forceinline__ uint64_t u64(const ThreadItem& s, uint32_t off) { return ldg64(s.tb + off); }
     static __device__ __forceinline__ LevelDesc desc(const ThreadItem& s, uint32_t L)
     {
         return load_desc(s.tb, s.desc_off, L);
     }
 };
-
-// 64-bit shift left whose amount saturates at 64 (PTX clamps shift amounts)
-__device__ __forceinline__ uint64_t shl_sat(uint64_t v, uint32_t n)
-{
-    uint64_t r;
-    asm("shl.b64 %0, %1, %2;" : "=l"(r) : "l"(v), "r"(n));
-    return r;
-}
 
 __device__ __forceinline__ uint32_t rec_t(const uint32_t* rec, uint32_t l)
 {
@@ -275,7 +274,7 @@ __device__ __forceinline__ uint32_t rec_t(const uint32_t* rec, uint32_t l)
 
 template <bool SM, int T>
 __device__ __forceinline__ void load_record(const BtLaunch& P, ThreadItem& s, const uint32_t* rec, uint32_t* stk,
-                                            uint64_t* av, uint64_t* spill)
+                                            uint32_t* av, uint32_t* spill)
 {
     using TB = Tab<SM>;
     s.orig = static_cast<uint64_t>(rec[0]) | (static_cast<uint64_t>(rec[1]) << 32);
@@ -287,17 +286,16 @@ __device__ __forceinline__ void load_record(const BtLaunch& P, ThreadItem& s, co
     s.n = TB::u32(s, H_N);
     s.desc_off = TB::u32(s, H_DESC);
     const uint32_t aw = TB::u32(s, H_AWORDS), init = TB::u32(s, H_INIT);
-    for (uint32_t w = 0; w < aw; ++w) av[w * T] = ldg64(s.tb + init + 2 * w);
+    for (uint32_t w = 0; w < aw; ++w) av[w * T] = ldg(s.tb + init + w);
     for (uint32_t l = 0; l < len; ++l) {
-        const LevelDesc d = TB::desc(s, l);
+        const uint32_t d0 = TB::u32(s, s.desc_off + 8 * l), d5 = TB::u32(s, s.desc_off + 8 * l + 5);
         const uint32_t t = rec_t(rec, l);
-        av[(d.aoff() + (t >> 6)) * T] &= ~(0xFull << (t & 60u));
-        stk[l * T] = (t << 21) | (TB::u32(s, d.d5 + t) & 0xFFFFFu);
+        av[((d0 >> 16) + (t >> 5)) * T] &= ~(0xFu << (t & 28u));
+        stk[l * T] = (t << 21) | (TB::u32(s, d5 + t) & 0xFFFFFu);
     }
     if (s.spilled) {
         const uint32_t* R = rec + P.rec_r_off;
-        for (uint32_t w = 0; w < P.max_kw; ++w)
-            spill[len * P.max_kw + w] = static_cast<uint64_t>(R[2 * w]) | (static_cast<uint64_t>(R[2 * w + 1]) << 32);
+        for (uint32_t w = 0; w < P.max_kw; ++w) spill[len * P.max_kw + w] = R[w];
     }
     s.L = len;
     s.base = len;
@@ -308,76 +306,78 @@ __device__ __forceinline__ void load_record(const BtLaunch& P, ThreadItem& s, co
     s.active = true;
 }
 
-// Candidate words of level L (not yet masked by the resume bit): the level's
-// pair-table row (frame sides & placed neighbours) & availability, or the
-// spilled remaining set.  stk/av are this thread's columns.
-template <int KW, bool SM, int T>
-__device__ __forceinline__ void level_candidates(const BtLaunch& P, const ThreadItem& s, const LevelDesc& d,
-                                                 uint32_t L, bool spilled, const uint32_t* stk, const uint64_t* av,
-                                                 const uint64_t* spill, uint64_t* x)
+// Candidate word w of level L from its pair-table row (frame sides & the first
+// two placed neighbours), the availability, and the side masks of further placed
+// neighbours (never present in row-major order).
+template <bool SM, int T>
+__device__ __forceinline__ uint32_t candidate_word(const ThreadItem& s, const LevelDesc& d, uint32_t row, uint32_t w,
+                                                   const uint32_t* stk, const uint32_t* av)
 {
-    const uint32_t kw = d.kw();
-    if (spilled) {
-        const uint64_t* sp = spill + L * P.max_kw;
-#pragma unroll
-        for (int w = 0; w < KW; ++w) x[w] = (uint32_t)w < kw ? sp[w] : 0ull;
-        return;
-    }
-    const uint32_t row = d.row(stk[d.level_a() * T], stk[d.level_b() * T]);
-    const uint64_t* a = av + d.aoff() * T;
-#pragma unroll
-    for (int w = 0; w < KW; ++w) x[w] = (uint32_t)w < kw ? Tab<SM>::u64(s, row + 2 * w) & a[w * T] : 0ull;
+    uint32_t x = Tab<SM>::u32(s, row + 1 + w) & av[(d.aoff() + w) * T];
     if (d.nextra()) {
-        const uint32_t ncol = Tab<SM>::u32(s, H_NCOL);
+        const uint32_t ncol = Tab<SM>::u32(s, H_NCOL), kw = d.kw();
         for (uint32_t j = 0; j < d.nextra(); ++j) {
             const uint32_t sd = d.extra_side(j);
             const uint32_t c = facing_colour(stk[d.extra_level(j) * T], sd);
-            const uint32_t* sm = s.tb + d.d4 + ((sd * ncol + c) * kw) * 2;
-#pragma unroll
-            for (int w = 0; w < KW; ++w)
-                if ((uint32_t)w < kw) x[w] &= ldg64(sm + 2 * w);
+            x &= ldg(s.tb + d.d4 + (sd * ncol + c) * kw + w);
         }
     }
+    return x;
 }
 
-// Masks the words below bit `start`, finds the first candidate t and whether
-// more candidates follow it.  Returns false when there is none.
-template <int KW>
-__device__ __forceinline__ bool first_candidate(uint64_t* x, uint32_t start, uint32_t* t, bool* more)
+// First candidate t >= start of level L, and whether more may follow it.  The
+// unspilled walk visits only the row's occupied words; `more` is exact within
+// t's word and counts any later occupied row word.  Returns false when none.
+template <bool SM, int T>
+__device__ __forceinline__ bool find_candidate(const BtLaunch& P, const ThreadItem& s, const LevelDesc& d, uint32_t L,
+                                               uint32_t start, bool spilled, const uint32_t* stk, const uint32_t* av,
+                                               const uint32_t* spill, uint32_t* t_out, bool* more_out)
 {
-    bool found = false;
-    uint32_t fw = 0;
-    uint64_t fx = 0;
-#pragma unroll
-    for (int w = 0; w < KW; ++w) {
-        const int sh = static_cast<int>(start) - 64 * w;
-        x[w] &= shl_sat(~0ull, static_cast<uint32_t>(sh > 0 ? sh : 0));
-        if (!found && x[w]) {
-            found = true;
-            fw = w;
-            fx = x[w];
+    const uint32_t sw = start >> 5;
+    const uint32_t low = shl32(~0u, start & 31u);
+    if (spilled) {
+        const uint32_t* sp = spill + L * P.max_kw;
+        const uint32_t kw = d.kw();
+        for (uint32_t w = sw; w < kw; ++w) {
+            uint32_t x = sp[w];
+            if (w == sw) x &= low;
+            if (x) {
+                *t_out = 32 * w + __ffs(x) - 1;
+                bool more = (x & (x - 1)) != 0;
+                for (uint32_t v = w + 1; v < kw && !more; ++v) more = sp[v] != 0;
+                *more_out = more;
+                return true;
+            }
+        }
+        return false;
+    }
+    const uint32_t row = d.row(stk[d.level_a() * T], stk[d.level_b() * T]);
+    uint32_t occ = Tab<SM>::u32(s, row) & shl32(~0u, sw);
+    while (occ) {
+        const uint32_t w = __ffs(occ) - 1;
+        occ &= occ - 1;
+        uint32_t x = candidate_word<SM, T>(s, d, row, w, stk, av);
+        if (w == sw) x &= low;
+        if (x) {
+            *t_out = 32 * w + __ffs(x) - 1;
+            *more_out = (x & (x - 1)) != 0 || occ != 0;
+            return true;
         }
     }
-    uint64_t rest = fx & (fx - 1);  // first word without t
-#pragma unroll
-    for (int w = 0; w < KW; ++w)
-        if ((uint32_t)w > fw) rest |= x[w];
-    *more = rest != 0;
-    *t = fw * 64 + __ffsll(fx) - 1;
-    return found;
+    return false;
 }
 
 // Goes up one level: gives back the piece placed there and resumes after it.
 template <bool SM, int T>
-__device__ __forceinline__ void pop_level(ThreadItem& s, const uint32_t* stk, uint64_t* av)
+__device__ __forceinline__ void pop_level(ThreadItem& s, const uint32_t* stk, uint32_t* av)
 {
     --s.L;
     const uint32_t e = stk[s.L * T];
     const uint32_t t = (e >> 21) & 0x3FFu;
     s.spilled = (e >> 20) & 1u;
     s.pop = !(e >> 31);
-    const LevelDesc dl = Tab<SM>::desc(s, s.L);
-    av[(dl.aoff() + (t >> 6)) * T] |= 0xFull << (t & 60u);
+    const uint32_t aoff = Tab<SM>::u32(s, s.desc_off + 8 * s.L) >> 16;
+    av[(aoff + (t >> 5)) * T] |= 0xFu << (t & 28u);
     s.start = t + 1;
 }
 
@@ -385,39 +385,38 @@ __device__ __forceinline__ void pop_level(ThreadItem& s, const uint32_t* stk, ui
 // inside the thread's record: place the next candidate of the current level,
 // or go up one level (without scanning when the level is known exhausted).
 // Returns false once the record is exhausted.
-template <int KW, bool SM, int T>
-__device__ __forceinline__ bool dfs_step(const BtLaunch& P, ThreadItem& s, uint32_t* stk, uint64_t* av,
-                                         uint64_t* spill, bool* solved)
+template <bool SM, int T>
+__device__ __forceinline__ bool dfs_step(const BtLaunch& P, ThreadItem& s, uint32_t* stk, uint32_t* av,
+                                         uint32_t* spill, bool* solved)
 {
     if (!s.pop) {
         const LevelDesc d = Tab<SM>::desc(s, s.L);
-        uint64_t x[KW];
-        level_candidates<KW, SM, T>(P, s, d, s.L, s.spilled != 0, stk, av, spill, x);
         uint32_t t;
         bool more;
-        if (first_candidate<KW>(x, s.start, &t, &more)) {
+        if (find_candidate<SM, T>(P, s, d, s.L, s.start, s.spilled != 0, stk, av, spill, &t, &more)) {
             const uint32_t ti = Tab<SM>::u32(s, d.d5 + t);
             if ((ti >> 20) & 1u) {
                 // select_piece with an identical mask that clears other candidates
                 // (emp_position_strategy.h:197-200): the level keeps its exact
                 // remaining set from now on
                 const uint32_t kw = d.kw();
-                if (!s.spilled) level_candidates<KW, SM, T>(P, s, d, s.L, false, stk, av, spill, x);
-                const uint32_t* ex = s.tb + d.d6 + t * kw * 2;
-                uint64_t* sp = spill + s.L * P.max_kw;
-                uint64_t rest = 0;
-#pragma unroll
-                for (int w = 0; w < KW; ++w)
-                    if ((uint32_t)w < kw) {
-                        sp[w] = x[w] & ldg64(ex + 2 * w);
-                        const int sh = static_cast<int>(t + 1) - 64 * w;
-                        rest |= sp[w] & shl_sat(~0ull, static_cast<uint32_t>(sh > 0 ? sh : 0));
-                    }
-                more = rest != 0;
+                uint32_t* sp = spill + s.L * P.max_kw;
+                const uint32_t* ex = s.tb + d.d6 + t * kw;
+                const uint32_t row = s.spilled ? 0u : d.row(stk[d.level_a() * T], stk[d.level_b() * T]);
+                const uint32_t tw = t >> 5;
+                bool rest = false;
+                for (uint32_t w = 0; w < kw; ++w) {
+                    uint32_t x = s.spilled ? sp[w] : candidate_word<SM, T>(s, d, row, w, stk, av);
+                    x &= ldg(ex + w);
+                    sp[w] = x;
+                    if (w > tw) rest |= x != 0;
+                    else if (w == tw) rest |= (x & shl32(~0u, (t & 31u) + 1)) != 0;
+                }
+                more = rest;
                 s.spilled = 1;
             }
-            uint64_t& aw = av[(d.aoff() + (t >> 6)) * T];
-            const uint64_t nib = 0xFull << (t & 60u);
+            uint32_t& aw = av[(d.aoff() + (t >> 5)) * T];
+            const uint32_t nib = 0xFu << (t & 28u);
             aw &= ~nib;
             stk[s.L * T] = (static_cast<uint32_t>(more) << 31) | (t << 21) | (s.spilled << 20) | (ti & 0xFFFFFu);
             ++s.nodes;
@@ -445,24 +444,22 @@ __device__ __forceinline__ bool dfs_step(const BtLaunch& P, ThreadItem& s, uint3
 // Keeps the lexicographically smallest solution path of each puzzle: in the
 // reference's visiting order (ascending candidate bit at every level) that is
 // its first solution.  The lock is held for a few hundred cycles; the wait for
-// it is bounded and a thread that gives up flags the record as unreliable.
+// it is bounded in time (first_lock_wait_ns of %globaltimer) and a thread that
+// gives up flags the record as missed, which the host reports as EMP_FIRST_LOST.
 template <int T>
 __device__ void record_solution(const BtLaunch& P, const ThreadItem& s, const uint32_t* stk)
 {
     FirstRecord* r = P.first_records + s.pz;
     atomicMin(&P.first_item[s.pz], (unsigned long long)s.orig);
     if (s.orig > *(volatile unsigned long long*)&P.first_item[s.pz]) return;
-    bool locked = false;
-    for (int tries = 0; tries < 4096; ++tries) {
-        if (atomicCAS(&r->lock, 0u, 1u) == 0u) {
-            locked = true;
-            break;
+    const uint64_t give_up = global_ns() + P.first_lock_wait_ns;
+    while (atomicCAS(&r->lock, 0u, 1u) != 0u) {
+        if (global_ns() > give_up) {
+            atomicExch(&r->missed, 1u);
+            atomicOr(P.status, EMP_DEV_FIRST_LOST);
+            return;
         }
         __nanosleep(64);
-    }
-    if (!locked) {
-        atomicExch(&r->missed, 1u);
-        return;
     }
     __threadfence();
     bool better = !r->has;
@@ -495,13 +492,12 @@ __device__ __forceinline__ void account(const BtLaunch& P, const ThreadItem& s)
 
 // Remaining candidates of level l (current level: from s.start unless it is
 // known exhausted; shallower levels: after their placed transition, when the
-// `more` bit says some remain), with `av` holding level l's entry availability.
-template <int KW, bool SM, int T>
+// `more` bit says some may remain), with `av` holding level l's entry availability.
+template <bool SM, int T>
 __device__ __forceinline__ bool level_has_work(const BtLaunch& P, const ThreadItem& s, uint32_t l, const uint32_t* stk,
-                                               const uint64_t* av, const uint64_t* spill, uint32_t* start_out,
+                                               const uint32_t* av, const uint32_t* spill, uint32_t* start_out,
                                                uint32_t* spilled_out)
 {
-    const LevelDesc d = Tab<SM>::desc(s, l);
     uint32_t start, spilled;
     bool maybe;
     if (l == s.L) {
@@ -517,21 +513,20 @@ __device__ __forceinline__ bool level_has_work(const BtLaunch& P, const ThreadIt
     *start_out = start;
     *spilled_out = spilled;
     if (!maybe) return false;
-    uint64_t x[KW];
-    level_candidates<KW, SM, T>(P, s, d, l, spilled != 0, stk, av, spill, x);
+    const LevelDesc d = Tab<SM>::desc(s, l);
     uint32_t t;
     bool more;
-    return first_candidate<KW>(x, start, &t, &more);
+    return find_candidate<SM, T>(P, s, d, l, start, spilled != 0, stk, av, spill, &t, &more);
 }
 
 template <bool SM, int T>
-__device__ __forceinline__ void toggle_piece(const ThreadItem& s, uint32_t l, const uint32_t* stk, uint64_t* av,
+__device__ __forceinline__ void toggle_piece(const ThreadItem& s, uint32_t l, const uint32_t* stk, uint32_t* av,
                                              bool give_back)
 {
-    const LevelDesc d = Tab<SM>::desc(s, l);
+    const uint32_t aoff = Tab<SM>::u32(s, s.desc_off + 8 * l) >> 16;
     const uint32_t t = (stk[l * T] >> 21) & 0x3FFu;
-    if (give_back) av[(d.aoff() + (t >> 6)) * T] |= 0xFull << (t & 60u);
-    else av[(d.aoff() + (t >> 6)) * T] &= ~(0xFull << (t & 60u));
+    if (give_back) av[(aoff + (t >> 5)) * T] |= 0xFu << (t & 28u);
+    else av[(aoff + (t >> 5)) * T] &= ~(0xFu << (t & 28u));
 }
 
 // Hands the remaining work of the thread's record to the next round: one
@@ -540,19 +535,19 @@ __device__ __forceinline__ void toggle_piece(const ThreadItem& s, uint32_t l, co
 // availability, and counts; pass 2 walks back down, writing records and taking
 // the pieces again, which leaves the state as it was.  Returns false when the
 // output queue is full (the thread then keeps the work).
-template <int KW, bool SM, int T>
-__device__ bool split_record(const BtLaunch& P, ThreadItem& s, uint32_t* stk, uint64_t* av, const uint64_t* spill)
+template <bool SM, int T>
+__device__ bool split_record(const BtLaunch& P, ThreadItem& s, uint32_t* stk, uint32_t* av, const uint32_t* spill)
 {
     uint32_t cnt = 0, start, spilled;
     for (uint32_t l = s.L + 1; l-- > s.base;) {
         if (l < s.L) toggle_piece<SM, T>(s, l, stk, av, true);
-        cnt += level_has_work<KW, SM, T>(P, s, l, stk, av, spill, &start, &spilled);
+        cnt += level_has_work<SM, T>(P, s, l, stk, av, spill, &start, &spilled);
     }
     const unsigned long long slot = cnt ? atomicAdd(P.out_tail, (unsigned long long)cnt) : 0ull;
     const bool fits = slot + cnt <= P.out_capacity;
     unsigned long long k = slot;
     for (uint32_t l = s.base; l <= s.L; ++l) {
-        if (level_has_work<KW, SM, T>(P, s, l, stk, av, spill, &start, &spilled)) {
+        if (level_has_work<SM, T>(P, s, l, stk, av, spill, &start, &spilled)) {
             if (fits) {
                 uint32_t* rec = P.out_rec + k * P.rec_words;
                 rec[0] = static_cast<uint32_t>(s.orig);
@@ -565,11 +560,7 @@ __device__ bool split_record(const BtLaunch& P, ThreadItem& s, uint32_t* stk, ui
                     rec[4 + (j >> 1)] = lo | (hi << 16);
                 }
                 if (spilled)
-                    for (uint32_t w = 0; w < P.max_kw; ++w) {
-                        const uint64_t v = spill[l * P.max_kw + w];
-                        rec[P.rec_r_off + 2 * w] = static_cast<uint32_t>(v);
-                        rec[P.rec_r_off + 2 * w + 1] = static_cast<uint32_t>(v >> 32);
-                    }
+                    for (uint32_t w = 0; w < P.max_kw; ++w) rec[P.rec_r_off + w] = spill[l * P.max_kw + w];
             } else if (k < P.out_capacity) {
                 P.out_rec[k * P.rec_words + 3] = 1u << 17;  // reserved slot that fits: mark empty
             }
@@ -580,7 +571,7 @@ __device__ bool split_record(const BtLaunch& P, ThreadItem& s, uint32_t* stk, ui
     return fits;
 }
 
-template <int KW, bool SM, int T, int kStepsPerFetch>
+template <bool SM, int T, int kStepsPerFetch>
 __global__ void __launch_bounds__(T) dfs_kernel(BtLaunch P)
 {
     const uint32_t tid = threadIdx.x, lane = tid & 31;
@@ -593,8 +584,8 @@ __global__ void __launch_bounds__(T) dfs_kernel(BtLaunch P)
     }
     // this thread's columns of the interleaved state
     uint32_t* stk = g_smem + P.smem_tab_words + tid;
-    uint64_t* av = reinterpret_cast<uint64_t*>(g_smem + P.smem_tab_words + P.max_levels * T) + tid;
-    uint64_t* spill = P.spill + (size_t)(blockIdx.x * T + tid) * P.max_levels * P.max_kw;
+    uint32_t* av = g_smem + P.smem_tab_words + P.max_levels * T + tid;
+    uint32_t* spill = P.spill + (size_t)(blockIdx.x * T + tid) * P.max_levels * P.max_kw;
     ThreadItem s;
     s.active = false;
     bool alive = true;
@@ -648,7 +639,7 @@ __global__ void __launch_bounds__(T) dfs_kernel(BtLaunch P)
         for (int step = 0; step < kStepsPerFetch; ++step) {
             if (s.active) {
                 bool solved = false;
-                if (dfs_step<KW, SM, T>(P, s, stk, av, spill, &solved)) {
+                if (dfs_step<SM, T>(P, s, stk, av, spill, &solved)) {
                     if (solved) {
                         record_solution<T>(P, s, stk);
                         if (P.sols) {
@@ -680,7 +671,7 @@ __global__ void __launch_bounds__(T) dfs_kernel(BtLaunch P)
 
         // ---- once the queue is empty, hand work back for the next round ----
         if (drained && P.item_budget && s.steps >= P.item_budget) {
-            if (split_record<KW, SM, T>(P, s, stk, av, spill)) {
+            if (split_record<SM, T>(P, s, stk, av, spill)) {
                 account(P, s);
                 s.active = false;
                 alive = false;
@@ -725,9 +716,11 @@ __global__ void reset_kernel(BtLaunch P, uint32_t n_puzzles)
         P.ctl->deadline = P.timeout_ns ? now + P.timeout_ns : 0ull;
         P.ctl->start_ns = now;
         P.ctl->first_found_ns = 0;
-        P.ctl->n_in = 0;
+        // a run whose first round takes its record count from the device starts from
+        // the count make_records left (graph runs, reused across selections)
+        P.ctl->n_in = P.n_in_from_ctl ? P.ctl->n_init : 0ull;
         P.ctl->rounds = 0;
-        P.ctl->records_in = P.n_in;
+        P.ctl->records_in = P.n_in_from_ctl ? P.ctl->n_init : P.n_in;
         P.ctl->records_out = 0;
     }
     if (i < n_puzzles) {
@@ -735,7 +728,7 @@ __global__ void reset_kernel(BtLaunch P, uint32_t n_puzzles)
         P.totals[2 * i] = 0;
         P.totals[2 * i + 1] = 0;
         P.first_item[i] = ~0ull;
-        P.first_records[i].lock = 0;
+        P.first_records[i].lock = P.first_lock_init;
         P.first_records[i].missed = 0;
         P.first_records[i].has = 0;
     }
@@ -744,8 +737,9 @@ __global__ void reset_kernel(BtLaunch P, uint32_t n_puzzles)
 // Initial records from split-depth prefixes (a strided selection of them).
 __global__ void make_records(const uint16_t* __restrict__ prefixes, const uint32_t* __restrict__ prefix_puzzle,
                              uint32_t depth, uint64_t first, uint64_t stride, uint64_t count, uint32_t rec_words,
-                             uint32_t* __restrict__ rec, const uint32_t* __restrict__ puzzle_depth)
+                             uint32_t* __restrict__ rec, const uint32_t* __restrict__ puzzle_depth, BtRunCtl* ctl)
 {
+    if (ctl && blockIdx.x == 0 && threadIdx.x == 0) ctl->n_init = count;
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < count;
          i += (uint64_t)gridDim.x * blockDim.x) {
         const uint64_t j = first + i * stride;
@@ -836,35 +830,21 @@ __global__ void record_prefix(const uint32_t* __restrict__ rec, uint32_t rec_wor
     for (uint32_t l = threadIdx.x; l < 256; l += blockDim.x) out[l] = l < len ? static_cast<uint16_t>(rec_t(r, l)) : 0xFFFFu;
 }
 
-template <int KW, int T>
+template <int T>
 const void* dfs_symbol(bool sm)
 {
-    return sm ? reinterpret_cast<const void*>(&dfs_kernel<KW, true, T, 32>)
-              : reinterpret_cast<const void*>(&dfs_kernel<KW, false, T, 32>);
-}
-
-template <int T>
-const void* dfs_symbol_for_t(uint32_t max_kw, bool sm)
-{
-    switch (max_kw) {
-        case 1: return dfs_symbol<1, T>(sm);
-        case 2: return dfs_symbol<2, T>(sm);
-        case 3: return dfs_symbol<3, T>(sm);
-        case 4: return dfs_symbol<4, T>(sm);
-        case 5: return dfs_symbol<5, T>(sm);
-        case 6: return dfs_symbol<6, T>(sm);
-        case 7: return dfs_symbol<7, T>(sm);
-        case 8: return dfs_symbol<8, T>(sm);
-        default: return max_kw <= 16 ? dfs_symbol<16, T>(sm) : nullptr;
-    }
+    return sm ? reinterpret_cast<const void*>(&dfs_kernel<true, T, 32>)
+              : reinterpret_cast<const void*>(&dfs_kernel<false, T, 32>);
 }
 
 const void* dfs_symbol_for(uint32_t max_kw, bool sm, uint32_t threads)
 {
+    if (max_kw > kMaxKindWords) return nullptr;
     switch (threads) {
-        case 64: return dfs_symbol_for_t<64>(max_kw, sm);
-        case 128: return dfs_symbol_for_t<128>(max_kw, sm);
-        case 256: return dfs_symbol_for_t<256>(max_kw, sm);
+        case 64: return dfs_symbol<64>(sm);
+        case 128: return dfs_symbol<128>(sm);
+        case 256: return dfs_symbol<256>(sm);
+        case 512: return dfs_symbol<512>(sm);
         default: return nullptr;
     }
 }
@@ -934,10 +914,10 @@ uint64_t scan_block_sum_words(uint64_t n) { return (n + kScanBlock - 1) / kScanB
 size_t dfs_smem_bytes(uint32_t max_levels, uint32_t max_avail_words, uint32_t threads, uint32_t tab_words)
 {
     return static_cast<size_t>(tab_words) * sizeof(uint32_t) +
-           (static_cast<size_t>(max_levels) * sizeof(uint32_t) + static_cast<size_t>(max_avail_words) * 8) * threads;
+           (static_cast<size_t>(max_levels) + static_cast<size_t>(max_avail_words)) * sizeof(uint32_t) * threads;
 }
 
-uint32_t record_words(uint32_t max_levels, uint32_t max_kw) { return 4 + (max_levels + 1) / 2 + 2 * max_kw; }
+uint32_t record_words(uint32_t max_levels, uint32_t max_kw) { return 4 + (max_levels + 1) / 2 + max_kw; }
 
 const void* dfs_kernel_symbol(uint32_t max_kw, bool smem_tables, uint32_t threads)
 {
@@ -961,12 +941,12 @@ cudaError_t launch_bt_reset(const BtLaunch& P, uint32_t n_puzzles, cudaStream_t 
 
 cudaError_t launch_make_records(const uint16_t* prefixes, const uint32_t* prefix_puzzle, uint32_t depth,
                                 uint64_t first, uint64_t stride, uint64_t count, uint32_t rec_words, uint32_t* rec,
-                                cudaStream_t stream, const uint32_t* puzzle_depth)
+                                cudaStream_t stream, const uint32_t* puzzle_depth, BtRunCtl* ctl)
 {
-    if (!count) return cudaSuccess;
-    const uint64_t blocks = std::min<uint64_t>((count + 255) / 256, 148ull * 32);
+    if (!count && !ctl) return cudaSuccess;
+    const uint64_t blocks = std::max<uint64_t>(1, std::min<uint64_t>((count + 255) / 256, 148ull * 32));
     make_records<<<(unsigned)blocks, 256, 0, stream>>>(prefixes, prefix_puzzle, depth, first, stride, count,
-                                                       rec_words, rec, puzzle_depth);
+                                                       rec_words, rec, puzzle_depth, ctl);
     return cudaGetLastError();
 }
 

@@ -12,6 +12,7 @@ enum : int {
     EMP_DEV_TIMEOUT = 1,    // the kernel passed its deadline and stopped
     EMP_DEV_ABORTED = 2,    // stopped early (deadline or cancel flag)
     EMP_DEV_SUPERSEDED = 8, // stop-at-first: subtrees after the first solution were cut
+    EMP_DEV_FIRST_LOST = 16,// a wait for a first-solution record ran out (the record missed a solution)
 };
 
 // Lexicographically smallest solution path of a puzzle (its first solution in
@@ -42,6 +43,7 @@ struct BtRunCtl {
     unsigned long long records_out;  // graph runs: records handed back for a next round
     unsigned long long start_ns;     // %globaltimer at the start of the run
     unsigned long long first_found_ns;  // %globaltimer when the first solution was found (0: none)
+    unsigned long long n_init;       // records of the run's first round (written by make_records)
 };
 
 struct BtLaunch {
@@ -49,9 +51,9 @@ struct BtLaunch {
     const uint64_t* puzzle_offset = nullptr;  // word offset of each puzzle blob
     uint32_t depth = 0;                       // split depth (prefix expansion)
     uint32_t max_levels = 0;                  // max pieces over the puzzles of the launch
-    uint32_t max_avail_words = 0;             // max 64-bit availability words (three kinds)
-    uint32_t max_kw = 0;                      // max 64-bit words of one kind
-    uint64_t* spill = nullptr;                // [threads][max_levels][max_kw] remaining sets
+    uint32_t max_avail_words = 0;             // max 32-bit availability words (three kinds)
+    uint32_t max_kw = 0;                      // max 32-bit candidate words of one kind
+    uint32_t* spill = nullptr;                // [threads][max_levels][max_kw] remaining sets
     uint32_t smem_tab_words = 0;              // > 0: single puzzle, hot tables staged in shared memory
     // work records of this round and of the next one
     const uint32_t* in_rec = nullptr;
@@ -79,6 +81,8 @@ struct BtLaunch {
     SolutionRecord* sols = nullptr;           // solution dumps: every solution found (null: not recorded)
     unsigned long long* sol_count = nullptr;
     unsigned long long sol_capacity = 0;
+    unsigned long long first_lock_wait_ns = 20000000ull;  // bound of a wait for a first-solution record
+    uint32_t first_lock_init = 0;             // value the records' locks start at (1: held by nobody; tests)
 };
 
 cudaError_t launch_expand(const BtLaunch& P, const uint16_t* parents, const uint32_t* parent_puzzle,
@@ -101,9 +105,11 @@ cudaError_t launch_expand_frozen(const BtLaunch& P, const uint16_t* parents, con
                                  cudaStream_t stream);
 // puzzle_depth (per puzzle, may be null): prefix length of each puzzle's records;
 // null = depth for all
+// ctl (may be null): receives count in ctl->n_init, the first round's record count
 cudaError_t launch_make_records(const uint16_t* prefixes, const uint32_t* prefix_puzzle, uint32_t depth,
                                 uint64_t first, uint64_t stride, uint64_t count, uint32_t rec_words, uint32_t* rec,
-                                cudaStream_t stream, const uint32_t* puzzle_depth = nullptr);
+                                cudaStream_t stream, const uint32_t* puzzle_depth = nullptr,
+                                BtRunCtl* ctl = nullptr);
 // Graph runs: the round controller (one thread) that turns this round's handed-back
 // records into the next round's input and sets the loop condition, and the copy of
 // those records into the input queue.

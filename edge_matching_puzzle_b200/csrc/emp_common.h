@@ -50,6 +50,9 @@ struct DeviceBuffer {
         bytes = n;
         return n ? cudaMalloc(&p, n) : cudaSuccess;
     }
+    // Keeps the allocation when it holds n bytes already (cudaFree synchronises
+    // the whole device, which would stall work queued on other streams).
+    cudaError_t reserve(size_t n) { return n <= bytes && p ? cudaSuccess : alloc(n); }
     template <class T>
     T* as() const { return static_cast<T*>(p); }
 };

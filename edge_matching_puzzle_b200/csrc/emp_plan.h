@@ -28,8 +28,11 @@ struct emp_bt_plan_t {
     std::vector<uint32_t> puzzle_depth;       // per puzzle split depth
     bool adaptive = false;                    // per puzzle split depths (split_subtrees)
     cudaStream_t capture_stream = nullptr;    // graph runs: stream the graph is captured on
+    cudaStream_t select_stream = nullptr;     // initial records of a selection are built here ...
+    cudaEvent_t ev_select = nullptr;          // ... and a run waits for this event before it starts
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
+    const void* graph_rec_init = nullptr;     // the initial-record buffer the graph was captured with
     bool graph_ran = false;
     // solution dumps: the expansion's level arrays (prefixes of length L at [L]) and
     // the solutions found
@@ -40,6 +43,7 @@ struct emp_bt_plan_t {
     uint64_t sol_capacity = 0;
     uint64_t n_all = 0, n_init = 0;
     bool sampled = false;
+    bool resumed = false;                     // initial records of a resumed search (emp_bt_resume)
     std::vector<unsigned long long> exp_nodes, exp_sols;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, evr0 = nullptr, evr1 = nullptr;
     bool ran = false;
@@ -53,12 +57,15 @@ struct emp_bt_plan_t {
         if (graph) cudaGraphDestroy(graph);
         graph_exec = nullptr;
         graph = nullptr;
+        graph_rec_init = nullptr;
     }
 
     ~emp_bt_plan_t()
     {
         drop_graph();
         if (capture_stream) cudaStreamDestroy(capture_stream);
+        if (select_stream) cudaStreamDestroy(select_stream);
+        if (ev_select) cudaEventDestroy(ev_select);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
         if (evr0) cudaEventDestroy(evr0);
@@ -74,10 +81,10 @@ struct emp_bt_plan_t {
         P.max_levels = max_levels;
         P.max_avail_words = max_avail;
         P.max_kw = max_kw;
-        P.spill = spill.as<uint64_t>();
+        P.spill = spill.as<uint32_t>();
         P.smem_tab_words = smem_tab_words;
         P.rec_words = rec_words;
-        P.rec_r_off = rec_words - 2 * max_kw;
+        P.rec_r_off = rec_words - max_kw;
         P.out_capacity = capacity;
         P.item_budget = budget;
         unsigned long long* c = counters.as<unsigned long long>();
@@ -98,6 +105,8 @@ struct emp_bt_plan_t {
         P.sol_count = sol_count.as<unsigned long long>();
         P.sol_capacity = sol_capacity;
         P.incomplete = incomplete.as<uint32_t>();
+        if (cfg.first_lock_wait_us) P.first_lock_wait_ns = 1000ull * cfg.first_lock_wait_us;
+        P.first_lock_init = cfg.hold_first_lock ? 1u : 0u;
         return P;
     }
 };

@@ -4,6 +4,8 @@
 #include <algorithm>
 #include <chrono>
 #include <fstream>
+#include <cstring>
+#include <cstdlib>
 #include <sstream>
 
 namespace edge_matching_puzzle {
@@ -66,6 +68,19 @@ emp_piece_set parse_pieces(const std::string& path)
     return set;
 }
 
+namespace {
+
+void check_order(const std::vector<uint16_t>& order, uint32_t n)
+{
+    std::vector<bool> used(n, false);
+    for (uint16_t p : order) {
+        if (p >= n || used[p]) throw emp_logic_error("The strategy does not list every position once", __LINE__, __FILE__);
+        used[p] = true;
+    }
+}
+
+}  // namespace
+
 std::unique_ptr<emp_strategy_generator> create_strategy_generator(const std::string& name, uint32_t width,
                                                                   uint32_t height)
 {
@@ -93,9 +108,81 @@ std::unique_ptr<emp_strategy_generator> create_strategy_generator(const std::str
             }
         }
     } else {
-        throw emp_logic_error("Unsupported strategy \"" + name + "\"", __LINE__, __FILE__);
+        std::ifstream text(name);
+        if (!text.is_open()) throw emp_logic_error("Unable to open file \"" + name + "\"", __LINE__, __FILE__);
+        std::string line;
+        for (uint32_t line_number = 1; order.size() < n && std::getline(text, line); ++line_number) {
+            if (line.empty() || line[0] == '#') continue;
+            const size_t comma = line.find(',');
+            if (comma == std::string::npos)
+                throw emp_logic_error("Missing ',' character in line " + std::to_string(line_number) + " : \"" + line +
+                                          "\"", __LINE__, __FILE__);
+            if (comma + 1 >= line.size())
+                throw emp_logic_error("Missing information after ',' character in line " +
+                                          std::to_string(line_number) + " : \"" + line + "\"", __LINE__, __FILE__);
+            const long x = std::atol(line.substr(0, comma).c_str()), y = std::atol(line.substr(comma + 1).c_str());
+            if (x < 0 || y < 0 || static_cast<uint32_t>(x) >= width || static_cast<uint32_t>(y) >= height)
+                throw emp_logic_error("Position (" + std::to_string(x) + "," + std::to_string(y) +
+                                          ") outside the puzzle in line " + std::to_string(line_number), __LINE__,
+                                      __FILE__);
+            order.push_back(static_cast<uint16_t>(y * width + x));
+        }
+        if (order.size() != n)
+            throw emp_logic_error("Incomplete strategy file \"" + name + "\" : " + std::to_string(order.size()) +
+                                      " < " + std::to_string(n), __LINE__, __FILE__);
+        check_order(order, n);
+        return std::make_unique<emp_strategy_generator>("text_generator", width, height, std::move(order));
     }
     return std::make_unique<emp_strategy_generator>(name, width, height, std::move(order));
+}
+
+std::unique_ptr<emp_strategy_generator> read_stream_strategy(std::istream& in, uint32_t width, uint32_t height)
+{
+    const uint32_t n = width * height;
+    std::vector<uint16_t> order;
+    for (uint32_t i = 0; i < n; ++i) {
+        uint32_t xy[2];
+        in.read(reinterpret_cast<char*>(xy), sizeof(xy));
+        if (!in) throw emp_logic_error("Truncated strategy stream", __LINE__, __FILE__);
+        if (xy[0] >= width || xy[1] >= height)
+            throw emp_logic_error("Position outside the puzzle in strategy stream", __LINE__, __FILE__);
+        order.push_back(static_cast<uint16_t>(xy[1] * width + xy[0]));
+    }
+    check_order(order, n);
+    return std::make_unique<emp_strategy_generator>("stream_generator", width, height, std::move(order));
+}
+
+std::vector<uint16_t> situation_transitions(const emp_piece_set& pieces, const emp_strategy_generator& strategy,
+                                            const std::string& situation)
+{
+    const uint32_t n = pieces.size();
+    const size_t wd = std::to_string(n).size() + 1;
+    if (situation.size() != n * wd)
+        throw emp_logic_error("Situation string of " + std::to_string(situation.size()) + " characters, expected " +
+                                  std::to_string(n * wd), __LINE__, __FILE__);
+    // kind index of each piece: its rank among the pieces with as many frame sides
+    std::vector<uint32_t> kind_index(n);
+    uint32_t seen[3] = {0, 0, 0};
+    for (uint32_t p = 0; p < n; ++p) {
+        uint32_t zeros = 0;
+        for (uint32_t s = 0; s < 4; ++s) zeros += pieces.colours[4 * p + s] == 0;
+        if (zeros > 2) throw emp_logic_error("Piece with more than two frame sides", __LINE__, __FILE__);
+        kind_index[p] = seen[zeros]++;
+    }
+    std::vector<uint16_t> out;
+    for (uint16_t pos : strategy.order()) {
+        const std::string cell = situation.substr(pos * wd, wd);
+        if (cell.substr(0, wd - 1) == std::string(wd - 1, '-')) break;
+        const char o = cell[wd - 1];
+        const char* letters = "NESW";
+        const char* at = std::strchr(letters, o);
+        if (!o || !at) throw emp_logic_error("Bad orientation '" + std::string(1, o) + "' in situation", __LINE__, __FILE__);
+        const long id = std::atol(cell.substr(0, wd - 1).c_str());
+        if (id < 1 || static_cast<uint32_t>(id) > n)
+            throw emp_logic_error("Bad piece id in situation: \"" + cell + "\"", __LINE__, __FILE__);
+        out.push_back(static_cast<uint16_t>((kind_index[id - 1] << 2) | static_cast<uint32_t>(at - letters)));
+    }
+    return out;
 }
 
 std::string situation_string(uint32_t width, uint32_t height, const uint32_t* cells)
@@ -147,12 +234,20 @@ void feature_CUDA_backtracker::run()
     cfg.stop_at_first = m_options.stop_at_first ? 1u : 0u;
     cfg.timeout_ms = m_options.timeout_ms;
     m_out << "Launch kernels" << std::endl;
-    const emp_status st = emp_bt_count(puzzle.get(), &cfg, &m_result);
-    if (st < 0) throw_abi("emp_bt_count", st, __LINE__);
+    emp_status st;
+    if (!m_options.initial_situation.empty()) {
+        const std::vector<uint16_t> sit = situation_transitions(m_pieces, m_strategy, m_options.initial_situation);
+        st = emp_bt_resume(puzzle.get(), sit.data(), static_cast<uint32_t>(sit.size()), &cfg, &m_result);
+        if (st < 0) throw_abi("emp_bt_resume", st, __LINE__);
+    } else {
+        st = emp_bt_count(puzzle.get(), &cfg, &m_result);
+        if (st < 0) throw_abi("emp_bt_count", st, __LINE__);
+    }
     // the first solution in visiting order, as the reference's backtracker prints it
     if (m_result.has_first_solution)
         m_out << situation_string(m_pieces.width, m_pieces.height, m_result.first_solution) << std::endl;
     if (st == EMP_INCOMPLETE) m_out << "Search stopped before the end (status " << m_result.status << ")" << std::endl;
+    if (st == EMP_FIRST_LOST) m_out << "First solution not recorded: " << emp_last_error() << std::endl;
     m_out << "End of algorithm" << std::endl;
     m_out << "Total situations explored : " << m_result.nodes << std::endl;
     m_out << "Nb solutions : " << m_result.solutions << std::endl;
@@ -215,12 +310,20 @@ void feature_new_strategy::run()
     std::vector<emp_bt_solution> sols(1024);
     uint64_t found = 0;
     emp_bt_result res{};
-    emp_status st = emp_bt_solutions(puzzle.get(), &cfg, sols.data(), sols.size(), &found, &res);
+    // --initial_situation: emp_strategy::set_initial_state, then the search from there
+    std::vector<uint16_t> sit;
+    if (!m_options.initial_situation.empty())
+        sit = situation_transitions(m_pieces, m_strategy, m_options.initial_situation);
+    auto dump = [&]() {
+        return emp_bt_resume_solutions(puzzle.get(), sit.data(), static_cast<uint32_t>(sit.size()), &cfg, sols.data(),
+                                       sols.size(), &found, &res);
+    };
+    emp_status st = dump();
     if (st == EMP_OK && found > sols.size()) {
         sols.resize(found);
-        st = emp_bt_solutions(puzzle.get(), &cfg, sols.data(), sols.size(), &found, &res);
+        st = dump();
     }
-    if (st != EMP_OK) throw_abi("emp_bt_solutions", st, __LINE__);
+    if (st != EMP_OK) throw_abi("emp_bt_resume_solutions", st, __LINE__);
     sols.resize(found);
     write_results_bin(m_dump_file, m_pieces, m_strategy, sols, res.nodes);
     m_out << "End of algorithm" << std::endl;
@@ -258,9 +361,12 @@ feature_if& factory_feature::create_feature(const std::string& feature_name, con
                                             const feature_options& options, std::ostream& out,
                                             const std::string& dump_file)
 {
-    if (feature_name == "new_strategy") {
-        // the reference's default order for this feature is the spiral (src/main.cpp:103-106)
-        if (!strategy) strategy = create_strategy_generator("spiral", pieces.width, pieces.height);
+    if (feature_name == "new_strategy" || feature_name == "new_text_strategy") {
+        // the reference's default orders for these features: the spiral, and the text
+        // strategy file strategy.txt (src/main.cpp:103-110)
+        if (!strategy)
+            strategy = create_strategy_generator(feature_name == "new_strategy" ? "spiral" : "strategy.txt",
+                                                 pieces.width, pieces.height);
         return *new feature_new_strategy(pieces, *strategy, dump_file, options, out);
     }
     if (feature_name == "CUDA_backtracker") {

@@ -23,6 +23,7 @@
 
 #include <cstdint>
 #include <iostream>
+#include <istream>
 #include <memory>
 #include <stdexcept>
 #include <string>
@@ -80,9 +81,26 @@ class emp_strategy_generator {
     std::vector<uint16_t> m_order;
 };
 
-// "basic" (row major) or "spiral"; anything else throws, as emp_strategy_generator_factory does.
+// "basic" (row major), "spiral", or else the name of a text strategy file, as
+// emp_strategy_generator_factory::create does (src/emp_strategy_generator_factory.cpp:
+// 24-39).  A text strategy (include/emp_text_strategy_generator.h:66-107) lists one
+// "x,y" position per line in visiting order; empty lines and lines starting with '#'
+// are skipped.  Throws emp_logic_error on a malformed or incomplete file, and when the
+// order does not list every position once.
 std::unique_ptr<emp_strategy_generator> create_strategy_generator(const std::string& name, uint32_t width,
                                                                   uint32_t height);
+
+// The stream strategy (include/emp_stream_strategy_generator.h): width*height (x, y)
+// pairs of 32-bit little-endian words read from a binary stream, the form in which a
+// results.bin file stores the order it was written with.
+std::unique_ptr<emp_strategy_generator> read_stream_strategy(std::istream& in, uint32_t width, uint32_t height);
+
+// Transitions (kind_index << 2 | orientation) of a situation string's pieces along
+// the strategy's order, up to its first empty position (include/emp_strategy.h:
+// 431-441 with include/situation_string_formatter.h:80-121).  Throws emp_logic_error
+// on a malformed string.
+std::vector<uint16_t> situation_transitions(const emp_piece_set& pieces, const emp_strategy_generator& strategy,
+                                            const std::string& situation);
 
 // The reference's board string: per position y*w+x the piece id right-aligned on
 // digits(w*h) characters plus N/E/S/W, or dashes when empty.  cells[pos] holds
@@ -97,6 +115,7 @@ class feature_if {
 
 // Settings the reference hard-codes; the defaults reproduce its behaviour.
 struct feature_options {
+    std::string initial_situation;  // new_strategy, CUDA_backtracker: resume from this situation string
     bool stop_at_first = false;     // backtracker: stop at the first solution found
     uint32_t split_depth = 0;       // backtracker: 0 = library default
     uint64_t push_budget = 0;       // glutton: stop after this many placements (0 = none)

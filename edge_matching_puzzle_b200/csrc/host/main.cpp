@@ -3,12 +3,16 @@
 //
 //   edge_matching_puzzle <definition.csv> <ressources> <feature_name> [--name=value ...]
 //
-// Feature names: CUDA_backtracker, CUDA_glutton_max, new_strategy (the exhaustive
-// search with its solution file, on the GPU).  Options the reference takes:
-//   --strategy=basic|spiral   position order (CUDA_backtracker: basic, new_strategy: spiral)
+// Feature names: CUDA_backtracker, CUDA_glutton_max, new_strategy and new_text_strategy
+// (the exhaustive search with its solution file, on the GPU).  Options the reference
+// takes:
+//   --strategy=basic|spiral|<file>  position order (CUDA_backtracker: basic, new_strategy:
+//                             spiral, new_text_strategy: the text file strategy.txt)
 //   --dump_file=<path>        new_strategy's solution file (default results.bin)
+//   --initial_situation=<s>   new_strategy, CUDA_backtracker: resume the search from the
+//                             situation string s (emp_strategy::set_initial_state)
 //   --enable_gui=...          accepted and ignored (there is no GUI here)
-//   --initial_situation, --hint   accepted and ignored
+//   --hint                    accepted and ignored
 // Settings the reference hard-codes, exposed here:
 //   --stop_at_first=true|false  --split_depth=N  --push_budget=N  --timeout_ms=N  --device=N
 // Errors print "ERROR : <what> at <file>:<line>" and exit with -1.
@@ -74,6 +78,7 @@ int main(int argc, char** argv)
         if (named.count("timeout_ms"))
             options.timeout_ms = static_cast<uint32_t>(parse_u64("timeout_ms", named["timeout_ms"]));
         if (named.count("device")) options.device = static_cast<int>(parse_u64("device", named["device"]));
+        if (named.count("initial_situation")) options.initial_situation = named["initial_situation"];
 
         const emp_piece_set pieces = parse_pieces(positional[0]);
         std::cout << pieces.size() << " pieces loaded" << std::endl;

@@ -16,6 +16,7 @@ LIB_PATH = os.path.join(HERE, "libemp_b200.so")
 
 EMP_OK = 0
 EMP_INCOMPLETE = 1
+EMP_FIRST_LOST = 2
 EMP_ERR_INVALID = -1
 EMP_ERR_UNSUPPORTED = -2
 EMP_ERR_CUDA = -3
@@ -58,6 +59,8 @@ class BtConfig(ctypes.Structure):
         ("split_subtrees", ctypes.c_uint32),
         ("use_graph", ctypes.c_uint32),
         ("stop_at_any", ctypes.c_uint32),
+        ("first_lock_wait_us", ctypes.c_uint32),
+        ("hold_first_lock", ctypes.c_uint32),
     ]
 
 
@@ -144,6 +147,11 @@ SIGNATURES = {
     "emp_puzzle_export_tables": (ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint32), ctypes.c_uint64,
                                                   u64p]),
     "emp_bt_count": (ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(BtConfig), ctypes.POINTER(BtResult)]),
+    "emp_bt_resume": (ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint16), ctypes.c_uint32,
+                                       ctypes.POINTER(BtConfig), ctypes.POINTER(BtResult)]),
+    "emp_bt_resume_solutions": (ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint16), ctypes.c_uint32,
+                                                 ctypes.POINTER(BtConfig), ctypes.POINTER(BtSolution),
+                                                 ctypes.c_uint64, u64p, ctypes.POINTER(BtResult)]),
     "emp_bt_count_batch": (ctypes.c_int32, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_uint32, ctypes.POINTER(BtConfig),
                                             ctypes.POINTER(BtResult)]),
     "emp_bt_plan_create": (ctypes.c_int32, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_uint32, ctypes.POINTER(BtConfig),
@@ -238,9 +246,9 @@ class NativePuzzle:
         return list(buf)
 
     def max_kind_words(self) -> int:
-        """64-bit words of the widest kind bitfield (4 bits per piece)."""
+        """32-bit words of the widest kind bitfield (4 bits per piece)."""
         i = self.info()
-        return (4 * max(i.nb_center, i.nb_border, i.nb_corner) + 63) // 64
+        return (4 * max(i.nb_center, i.nb_border, i.nb_corner) + 31) // 32
 
     def table_bytes(self) -> int:
         return 4 * len(self.export_tables())
@@ -264,6 +272,29 @@ def bt_count(puzzle: NativePuzzle, **kw) -> BtResult:
     cfg = bt_config(**kw)
     check(load().emp_bt_count(puzzle.handle, ctypes.byref(cfg), ctypes.byref(r)))
     return r
+
+
+def bt_resume(puzzle: NativePuzzle, situation: Sequence[int], **kw) -> BtResult:
+    """emp_bt_resume: the search resumed from a partial situation (the transitions placed
+    at the first levels of the puzzle's order), as --initial_situation does."""
+    r = BtResult()
+    cfg = bt_config(**kw)
+    arr = (ctypes.c_uint16 * max(1, len(situation)))(*situation)
+    check(load().emp_bt_resume(puzzle.handle, arr, len(situation), ctypes.byref(cfg), ctypes.byref(r)))
+    return r
+
+
+def bt_resume_solutions(puzzle: NativePuzzle, situation: Sequence[int], capacity: int = 4096, **kw):
+    """emp_bt_resume_solutions: (found, [(node_index, board)], result) of the resumed search."""
+    out = (BtSolution * max(capacity, 1))()
+    found = ctypes.c_uint64()
+    res = BtResult()
+    cfg = bt_config(**kw)
+    arr = (ctypes.c_uint16 * max(1, len(situation)))(*situation)
+    check(load().emp_bt_resume_solutions(puzzle.handle, arr, len(situation), ctypes.byref(cfg), out, capacity,
+                                         ctypes.byref(found), ctypes.byref(res)))
+    n = min(found.value, capacity)
+    return found.value, [(out[i].node_index, list(out[i].board)) for i in range(n)], res
 
 
 def bt_count_batch(puzzles: Sequence[NativePuzzle], **kw) -> List[BtResult]:
@@ -469,7 +500,7 @@ class BtPlan:
         """32-bit words per work record (header, prefix, remaining set)."""
         n = max(p.n for p in self.puzzles)
         kw = max(p.max_kind_words() for p in self.puzzles)
-        return 4 + (n + 1) // 2 + 2 * kw
+        return 4 + (n + 1) // 2 + kw
 
     def close(self):
         if getattr(self, "handle", None):

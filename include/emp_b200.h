@@ -36,6 +36,9 @@ extern "C" {
 typedef int32_t emp_status;
 #define EMP_OK 0
 #define EMP_INCOMPLETE 1          /* stopped by the timeout or a cancel: partial counts */
+#define EMP_FIRST_LOST 2          /* counts complete and exact, but the first solution's board was not
+                                     recorded: a thread's wait for the puzzle's first-solution record
+                                     ran past first_lock_wait_us (has_first_solution is then 0) */
 #define EMP_ERR_INVALID (-1)      /* bad argument or malformed puzzle */
 #define EMP_ERR_UNSUPPORTED (-2)  /* valid input outside what the kernels support */
 #define EMP_ERR_CUDA (-3)         /* CUDA runtime error (no device, launch failure...) */
@@ -98,7 +101,7 @@ emp_status emp_puzzle_export_tables(emp_puzzle puzzle, uint32_t *out, uint64_t c
 
 typedef struct emp_bt_config {
     uint32_t split_depth;        /* levels expanded before subtrees go to threads; 0 = auto */
-    uint32_t threads_per_block;  /* 64, 128 or 256; 0 = the size with the most resident warps */
+    uint32_t threads_per_block;  /* 64, 128, 256 or 512; 0 = the size with the most resident warps */
     uint32_t blocks_per_sm;      /* 0 = as many as fit */
     uint32_t stop_at_first;      /* 1: stop once the reference's first solution is known */
     uint64_t reserved_budget;    /* unused, keep 0 */
@@ -122,6 +125,11 @@ typedef struct emp_bt_config {
                                     0: the host starts each round */
     uint32_t stop_at_any;        /* 1: stop the whole run at the first solution found by any thread
                                     (time to a first solution; counts are then partial) */
+    uint32_t first_lock_wait_us; /* bound of a thread's wait for its puzzle's first-solution record,
+                                    which another thread holds for a few hundred cycles; 0 = 20000.
+                                    A wait that runs out reports EMP_FIRST_LOST for the puzzle */
+    uint32_t hold_first_lock;    /* testing only: 1 = every first-solution record starts locked by
+                                    nobody, so each wait runs out (exercises EMP_FIRST_LOST) */
 } emp_bt_config;
 
 typedef struct emp_bt_result {
@@ -151,6 +159,19 @@ typedef struct emp_bt_result {
  * below the split depth). */
 emp_status emp_bt_count(emp_puzzle puzzle, const emp_bt_config *config, emp_bt_result *result);
 
+/* The same search resumed from a partial situation, as the reference's
+ * --initial_situation parameter does for new_strategy: emp_strategy::set_initial_state
+ * followed by specific_run (include/emp_strategy.h:418-467, 343-410).  situation[l] is
+ * the transition t = kind_index<<2 | orientation placed at level l of the puzzle's
+ * order, for l < placed (the situation string's pieces up to its first empty position
+ * in that order).  As in the reference, the search restarts the last placed level
+ * from its first candidate, continues with the candidates every shallower level has
+ * left after the situation's piece, and ends when level 1 is exhausted; nodes and
+ * solutions count that search alone.  placed <= 1 is a whole search (emp_bt_count).
+ * A situation piece that the reference's order cannot reach is EMP_ERR_INVALID. */
+emp_status emp_bt_resume(emp_puzzle puzzle, const uint16_t *situation, uint32_t placed,
+                         const emp_bt_config *config, emp_bt_result *result);
+
 /* Same for many puzzles in one persistent launch; results[i] per puzzle. */
 emp_status emp_bt_count_batch(const emp_puzzle *puzzles, uint32_t count, const emp_bt_config *config,
                               emp_bt_result *results);
@@ -168,9 +189,18 @@ typedef struct emp_bt_solution {
  * emp_strategy writes to results.bin (include/emp_strategy.h:367-375).  The search runs
  * without handing work between threads (each subtree is searched in order by one
  * thread), so it is slower than emp_bt_count on large trees.  *found receives the
- * number of solutions; the first min(found, capacity) are written to out. */
+ * number of solutions; out receives the first min(found, capacity) of them in the
+ * reference's order (when found > capacity the search runs a second time keeping all
+ * of them, at most 2^20, to rank them; more than that fails with EMP_ERR_UNSUPPORTED). */
 emp_status emp_bt_solutions(emp_puzzle puzzle, const emp_bt_config *config, emp_bt_solution *out, uint64_t capacity,
                             uint64_t *found, emp_bt_result *result);
+
+/* emp_bt_solutions of the search resumed from a partial situation (emp_bt_resume):
+ * what the reference's new_strategy with --initial_situation writes to results.bin,
+ * each solution with the placements of the resumed search up to it. */
+emp_status emp_bt_resume_solutions(emp_puzzle puzzle, const uint16_t *situation, uint32_t placed,
+                                   const emp_bt_config *config, emp_bt_solution *out, uint64_t capacity,
+                                   uint64_t *found, emp_bt_result *result);
 
 /* Split form of the batch call: plan (upload + prefix expansion), run (kernel
  * launch on a stream, asynchronous), results (synchronise + download). */
@@ -206,7 +236,7 @@ typedef struct emp_bt_tune_result {
 /* Chooses the launch parameters for a set of puzzles by timing short runs on the
  * device.  Starting from base (NULL = defaults), it tunes one field at a time, keeping
  * each field's fastest value before moving on:
- *   threads_per_block   64, 128, 256
+ *   threads_per_block   64, 128, 256, 512
  *   split_subtrees      per-puzzle split targets (batches of several puzzles) or
  *   split_depth         split depths (a single puzzle)
  *   split_budget        steps before a thread hands work back

@@ -4,6 +4,9 @@ The CUDA path is reached through the C ABI (libemp_b200.so); the oracle is the j
 """
 from __future__ import annotations
 
+import hashlib
+import json
+import os
 import random
 
 import pytest
@@ -13,6 +16,9 @@ from edge_matching_puzzle_b200.puzzle import Puzzle, board_string, generate, row
 from oracle.oracle import OraclePuzzle
 
 pytestmark = pytest.mark.gpu
+
+with open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "ref_counts.json")) as _f:
+    REF_RECORDS = json.load(_f)["records"]
 
 
 def _check(pz: Puzzle, order=None, depths=(None,), **kw):
@@ -153,16 +159,20 @@ def test_8x8_largest_seed_subtree_sample():
     assert res.nodes == sum(nodes) and res.solutions == sum(sols)
 
 
-@pytest.mark.parametrize("rank", range(5))
-def test_8x8_full_count_against_cpu_golden(config_counts, rank):
-    """Whole exhaustive count of an 8x8 workload seed (the five smallest trees, 3.8e9 to
-    4.8e10 placements) equals the CPU oracle's count."""
-    recs = sorted((r for r in config_counts["records"] if r["config"] == "8x8"), key=lambda r: r["nodes"])
-    rec = recs[rank]
-    pz = generate(8, 8, 4, 8, rec["seed"])
-    r = native.bt_count(native.NativePuzzle(8, 8, pz.colors), split_depth=12, timeout_ms=60000)
+CPU_COUNTED_8X8 = [0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 14, 15]
+
+
+@pytest.mark.parametrize("seed", CPU_COUNTED_8X8)
+def test_8x8_full_count_against_cpu_golden(config_counts, seed):
+    """Whole exhaustive count of every 8x8 workload seed the CPU could count (all but
+    seed 13, 1.5e13 placements: see test_8x8_largest_seed_subtree_sample) equals the
+    CPU oracle's count: 3.8e9 to 1.27e12 placements per seed, 2.6e12 in all."""
+    rec = [r for r in config_counts["records"] if r["config"] == "8x8" and r["seed"] == seed][0]
+    pz = generate(8, 8, 4, 8, seed)
+    r = native.bt_count(native.NativePuzzle(8, 8, pz.colors), split_depth=12, timeout_ms=240000)
     assert r.status == native.EMP_OK
     assert (r.nodes, r.solutions) == (rec["nodes"], rec["solutions"])
+    assert bool(r.has_first_solution) == (rec["solutions"] > 0)
 
 
 def test_split_depth_invariance():
@@ -251,3 +261,111 @@ def test_solution_dump_matches_oracle_results_bin(tmp_path, seed):
         found, sols, res = native.bt_solutions(npz, capacity=1 << 16, split_depth=min(4, w * h - 2))
         assert found == want.solutions and res.nodes == want.nodes
         assert _results_bin(pz, order, sols, res.nodes) == open(path, "rb").read()
+
+
+def _ref_order(rec, pz):
+    return spiral_order(pz.width, pz.height) if rec["order"] == "spiral" else row_major_order(pz.width, pz.height)
+
+
+@pytest.mark.parametrize("group", ["examples", "config0", "random", "quirk", "batch"])
+def test_counts_equal_reference_build(group):
+    """Counts of the puzzles that the reference's own emp_strategy counted (built from
+    its sources into oracle/_ref; tests/golden/ref_counts.json): identical-piece masks,
+    cross-kind twin masks, masks written outside a bitfield, row-major and spiral."""
+    recs = [r for r in REF_RECORDS if r["group"] == group]
+    assert recs
+    for rec in recs:
+        pz = Puzzle.from_csv(rec["csv"])
+        npz = native.NativePuzzle(pz.width, pz.height, pz.colors, order=_ref_order(rec, pz))
+        r = native.bt_count(npz, split_depth=min(6, pz.nb_pieces - 1))
+        assert r.status == native.EMP_OK
+        assert (r.nodes, r.solutions) == (rec["nodes"], rec["solutions"]), rec["name"]
+
+
+@pytest.mark.parametrize("group", ["examples", "config0", "quirk"])
+def test_results_bin_equals_reference_build(group):
+    """Every solution of the GPU solution dump, written as results.bin, has the SHA-256
+    of the file the reference's own build wrote."""
+    for rec in [r for r in REF_RECORDS if r["group"] == group and r["solutions"] <= 4096]:
+        pz = Puzzle.from_csv(rec["csv"])
+        order = _ref_order(rec, pz)
+        npz = native.NativePuzzle(pz.width, pz.height, pz.colors, order=order)
+        found, sols, res = native.bt_solutions(npz, capacity=4096, split_depth=min(4, pz.nb_pieces - 2))
+        assert found == rec["solutions"] and res.nodes == rec["nodes"], rec["name"]
+        digest = hashlib.sha256(_results_bin(pz, order, sols, res.nodes)).hexdigest()
+        assert digest == rec["results_sha256"], rec["name"]
+
+
+def test_solution_dump_capacity_keeps_reference_order(reference_vectors, tmp_path):
+    """With fewer slots than solutions, emp_bt_solutions returns the FIRST solutions in
+    the reference's order (the 4x4 example has 12), not the first ones to arrive."""
+    pz = Puzzle.from_csv(reference_vectors["puzzles"]["4_4"])
+    order = spiral_order(4, 4)
+    npz = native.NativePuzzle(4, 4, pz.colors, order=order)
+    found_all, all_sols, res = native.bt_solutions(npz, capacity=64, split_depth=3)
+    assert found_all == 12
+    want_path = str(tmp_path / "oracle.bin")
+    want, _ = OraclePuzzle(4, 4, pz.colors).run(order=order, results_bin=want_path)
+    assert _results_bin(pz, order, all_sols, res.nodes) == open(want_path, "rb").read()
+    for cap in (1, 5, 11):
+        found, sols, _ = native.bt_solutions(npz, capacity=cap, split_depth=3)
+        assert found == 12 and len(sols) == cap
+        assert sols == all_sols[:cap]
+    assert all_sols[0][0] == want.first_solution_nodes
+    assert all_sols[0][1][:16] == list(want.first_board)[:16]
+
+
+def test_lost_first_solution_record_is_reported():
+    """A first-solution record whose lock wait runs out is reported as EMP_FIRST_LOST
+    (exact counts, no board), not as a run without a first solution.  The test holds
+    every record's lock from the start (a lock nothing releases) with a 1 us bound."""
+    import ctypes
+    pz = generate(5, 5, 3, 5, 0)
+    want, _ = OraclePuzzle(5, 5, pz.colors).run()
+    npz = native.NativePuzzle(5, 5, pz.colors)
+    cfg = native.bt_config(split_depth=6, hold_first_lock=1, first_lock_wait_us=1)
+    r = native.BtResult()
+    st = native.load().emp_bt_count(npz.handle, ctypes.byref(cfg), ctypes.byref(r))
+    assert st == native.EMP_FIRST_LOST and r.status == native.EMP_FIRST_LOST
+    assert not r.has_first_solution
+    assert (r.nodes, r.solutions) == (want.nodes, want.solutions)
+    ok = native.bt_count(npz, split_depth=6)
+    assert ok.status == native.EMP_OK and ok.has_first_solution
+
+
+def test_resume_equals_reference_build():
+    """emp_bt_resume (--initial_situation) against the reference's own set_initial_state +
+    specific_run on mid-board situations, row-major and spiral."""
+    from edge_matching_puzzle_b200.puzzle import parse_board_string, situation_transitions
+    recs = [r for r in REF_RECORDS if r["group"] == "resume"]
+    assert recs
+    for rec in recs:
+        pz = Puzzle.from_csv(rec["csv"])
+        order = _ref_order(rec, pz)
+        trans = situation_transitions(pz, order, parse_board_string(pz.width, pz.height, rec["initial_situation"]))
+        npz = native.NativePuzzle(pz.width, pz.height, pz.colors, order=order)
+        for budget in (0, 64):  # work handed between threads, or not
+            r = native.bt_resume(npz, trans, split_budget=budget)
+            assert r.status == native.EMP_OK
+            assert (r.nodes, r.solutions) == (rec["nodes"], rec["solutions"]), rec["name"]
+
+
+def test_resume_rejects_unreachable_situation():
+    pz = generate(5, 5, 3, 5, 0)
+    npz = native.NativePuzzle(5, 5, pz.colors)
+    with pytest.raises(native.EmpError):
+        native.bt_resume(npz, [0, 0, 0])  # the same corner twice
+
+
+def test_resume_solutions_results_bin_equals_reference_build():
+    """new_strategy with --initial_situation: the resumed search's results.bin (solutions
+    with the resumed search's node indices) has the SHA-256 of the reference's file."""
+    from edge_matching_puzzle_b200.puzzle import parse_board_string, situation_transitions
+    for rec in [r for r in REF_RECORDS if r["group"] == "resume" and r["solutions"] <= 4096]:
+        pz = Puzzle.from_csv(rec["csv"])
+        order = _ref_order(rec, pz)
+        trans = situation_transitions(pz, order, parse_board_string(pz.width, pz.height, rec["initial_situation"]))
+        npz = native.NativePuzzle(pz.width, pz.height, pz.colors, order=order)
+        found, sols, res = native.bt_resume_solutions(npz, trans, capacity=4096)
+        assert found == rec["solutions"] and res.nodes == rec["nodes"], rec["name"]
+        assert hashlib.sha256(_results_bin(pz, order, sols, res.nodes)).hexdigest() == rec["results_sha256"], rec["name"]

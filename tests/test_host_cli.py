@@ -59,7 +59,7 @@ def test_piece_count_mismatch(cli, tmp_path, reference_vectors):
 
 
 @pytest.mark.parametrize("args,msg", [
-    (["--strategy=zigzag"], 'Unsupported strategy "zigzag"'),
+    (["--strategy=zigzag"], 'Unable to open file "zigzag"'),
     (["--colour=3"], 'Unknown parameter "colour"'),
     (["--stop_at_first=maybe"], 'Bad boolean value "maybe"'),
 ])
@@ -122,5 +122,61 @@ def test_new_strategy_reports_errors_like_the_other_features(cli, tmp_path, refe
     path = tmp_path / "3_3.txt"
     path.write_text(reference_vectors["puzzles"]["3_3"])
     rc, out = run(cli, str(path), "ressources", "new_strategy", "--strategy=zigzag", f"--dump_file={tmp_path / 'r.bin'}")
-    assert rc == 255 and 'Unsupported strategy "zigzag"' in out[-1]
+    assert rc == 255 and 'Unable to open file "zigzag"' in out[-1]
     assert not (tmp_path / "r.bin").exists()
+
+
+def _write_strategy(path, positions, comment=True):
+    lines = (["# x,y of each position in visiting order"] if comment else []) + [f"{x},{y}" for x, y in positions]
+    path.write_text("\n".join(lines) + "\n")
+
+
+@pytest.mark.parametrize("content,msg", [
+    ("0,0\n1\n", "Missing ',' character in line 2"),
+    ("0,0\n1,\n", "Missing information after ',' character in line 2"),
+    ("0,0\n1,0\n", "Incomplete strategy file"),
+    ("0,0\n0,0\n0,1\n0,2\n1,1\n1,2\n2,0\n2,1\n2,2\n", "does not list every position once"),
+])
+def test_text_strategy_errors(cli, example, tmp_path, content, msg):
+    """include/emp_text_strategy_generator.h:66-107: the text strategy's error lines."""
+    strat = tmp_path / "strat.txt"
+    strat.write_text(content)
+    rc, out = run(cli, example("3_3"), "ressources", "CUDA_backtracker", f"--strategy={strat}")
+    assert rc == 255 and msg in out[-1], out
+
+
+def test_bad_initial_situation(cli, example):
+    rc, out = run(cli, example("3_3"), "ressources", "CUDA_backtracker", "--initial_situation=1N2N")
+    assert rc == 255 and "Situation string of 4 characters, expected 18" in out[-1]
+
+
+@pytest.mark.gpu
+def test_new_text_strategy_reads_strategy_txt(cli, reference_vectors, tmp_path):
+    """new_text_strategy takes its order from ./strategy.txt: the spiral written as text
+    gives the reference's own new_strategy results.bin."""
+    import base64
+    from edge_matching_puzzle_b200.puzzle import spiral_order
+    (tmp_path / "4_4.txt").write_text(reference_vectors["puzzles"]["4_4"])
+    _write_strategy(tmp_path / "strategy.txt", [(p % 4, p // 4) for p in spiral_order(4, 4)])
+    r = subprocess.run([cli, "4_4.txt", "ressources", "new_text_strategy", "--dump_file=r.bin"], capture_output=True,
+                       text=True, timeout=300, cwd=tmp_path)
+    assert r.returncode == 0, r.stdout
+    golden = reference_vectors["new_strategy"]["4_4"]
+    assert (tmp_path / "r.bin").read_bytes() == base64.b64decode(golden["results_bin_b64"])
+
+
+@pytest.mark.gpu
+def test_new_strategy_initial_situation_matches_reference_build(cli, tmp_path):
+    """--initial_situation: totals and results.bin of the reference's own build resumed
+    from the same situation (tests/golden/ref_counts.json)."""
+    import hashlib
+    import json
+    recs = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "ref_counts.json")))["records"]
+    for rec in [r for r in recs if r["group"] == "resume"][:6]:
+        (tmp_path / "p.txt").write_text(rec["csv"])
+        dump = tmp_path / "r.bin"
+        rc, out = run(cli, str(tmp_path / "p.txt"), "ressources", "new_strategy", f"--strategy={rec['order']}",
+                      f"--initial_situation={rec['initial_situation']}", f"--dump_file={dump}")
+        assert rc == 0, out
+        assert f"Total situations explored : {rec['nodes']}" in out and f"Nb solutions : {rec['solutions']}" in out
+        assert hashlib.sha256(dump.read_bytes()).hexdigest() == rec["results_sha256"], rec["name"]
