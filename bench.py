@@ -728,8 +728,7 @@ def main():
                          "frac": dram_alg / (launch_ms / 1000) / 1e9 / peaks["hbm_gbs"],
                          "traffic": DFS_LAUNCH_DRAM_BYTES,
                          "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one dfs_kernel round "
-                                           "(seed-0 slice, same grid and table staging; caches flushed by ncu), "
-                                           "profiles/dfs_kernel_8x8_seed0_ncu_full.md",
+                                           "(seed-0 slice, same grid and table staging; caches flushed by ncu)",
                          "peak_source": peak_kind,
                          "note": "dfs_kernel keeps its state on chip; DRAM only carries work records, so the "
                                  "on-chip roofline below is the binding one"},

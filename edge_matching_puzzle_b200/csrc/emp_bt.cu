@@ -382,14 +382,19 @@ __device__ __forceinline__ void pop_level(ThreadItem& s, const uint32_t* stk, ui
 }
 
 // One step of emp_strategy::specific_run (include/emp_strategy.h:352-401)
-// inside the thread's record: place the next candidate of the current level,
-// or go up one level (without scanning when the level is known exhausted).
-// Returns false once the record is exhausted.
+// inside the thread's record: go up past the levels known to be exhausted, then
+// place the next candidate of the current level, or go up one level when it has
+// none.  Doing the known pops and the next try in the same step keeps the lanes
+// of a warp on the same (try) path.  Returns false once the record is exhausted.
 template <bool SM, int T>
 __device__ __forceinline__ bool dfs_step(const BtLaunch& P, ThreadItem& s, uint32_t* stk, uint32_t* av,
                                          uint32_t* spill, bool* solved)
 {
-    if (!s.pop) {
+    while (s.pop) {
+        if (s.L == s.base) return false;
+        pop_level<SM, T>(s, stk, av);
+    }
+    {
         const LevelDesc d = Tab<SM>::desc(s, s.L);
         uint32_t t;
         bool more;

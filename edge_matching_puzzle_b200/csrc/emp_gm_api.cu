@@ -8,7 +8,6 @@
 #include <algorithm>
 #include <chrono>
 #include <cstring>
-#include <mutex>
 #include <string>
 #include <vector>
 
@@ -189,7 +188,8 @@ extern "C" emp_status emp_glutton_max(emp_puzzle puzzle, const emp_gm_config* co
 //   cc      32 colours x 4 sides x 32 words
 //   infos   triangular level stack for 256 positions: 256*257/2 infos x 32 words
 // 4,232,448 bytes in all, enough for every puzzle the library accepts (at most
-// 256 pieces, colour ids up to 31).
+// 256 pieces; colour ids up to 30, which build_model enforces, so the colour check
+// below is a second guard that a valid puzzle never trips).
 namespace {
 
 constexpr size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
@@ -202,11 +202,6 @@ constexpr size_t kOffInfos = align256(kOffCc + sizeof(uint32_t) * kNoAllocMaxCol
 constexpr size_t kNoAllocBytes =
     align256(kOffInfos + sizeof(uint32_t) * 32 * (size_t(kNoAllocMaxPieces) * (kNoAllocMaxPieces + 1) / 2));
 static_assert(kNoAllocBytes == 4232448, "scratch size stated above");
-constexpr int kNoAllocMaxDevices = 64;
-
-std::mutex g_noalloc_mu;
-unsigned char* g_noalloc_ptr[kNoAllocMaxDevices] = {};
-
 }  // namespace
 
 static __device__ __align__(256) unsigned char g_gm_scratch[kNoAllocBytes];
@@ -229,24 +224,21 @@ extern "C" emp_status emp_glutton_max_noalloc(emp_puzzle puzzle, const emp_gm_co
                                              std::to_string(kNoAllocMaxColours));
     int dev = 0;
     EMP_TRY(emp::select_device(cfg.device, &dev));
-    if (dev >= kNoAllocMaxDevices) return fail(EMP_ERR_UNSUPPORTED, "emp_glutton_max_noalloc: device ordinal above 63");
     cudaDeviceProp prop;
     CUDA_TRY(cudaGetDeviceProperties(&prop, dev));
     if (emp::gm_smem_bytes() > static_cast<size_t>(prop.sharedMemPerBlockOptin))
         return fail(EMP_ERR_UNSUPPORTED, "glutton max level state does not fit shared memory");
 
-    // One-time set-up per device, with that device current: look up the device
-    // address of the scratch array (this is what loads it onto the device).
+    // The device address of the scratch array on the current device, looked up on
+    // every call (no allocation; the first look-up on a device loads the array onto
+    // it).  A cached address would go stale after cudaDeviceReset, which loads the
+    // module again, possibly elsewhere.
     unsigned char* base = nullptr;
     {
-        std::lock_guard<std::mutex> lock(g_noalloc_mu);
-        if (!g_noalloc_ptr[dev]) {
-            void* p = nullptr;
-            cudaError_t e = cudaGetSymbolAddress(&p, g_gm_scratch);
-            if (e != cudaSuccess) return emp::cuda_fail(e, "emp_glutton_max_noalloc: scratch address look-up");
-            g_noalloc_ptr[dev] = static_cast<unsigned char*>(p);
-        }
-        base = g_noalloc_ptr[dev];
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_gm_scratch);
+        if (e != cudaSuccess) return emp::cuda_fail(e, "emp_glutton_max_noalloc: scratch address look-up");
+        base = static_cast<unsigned char*>(p);
     }
 
     const uint32_t S = m.n;

@@ -370,12 +370,17 @@ emp_status emp_glutton_max(emp_puzzle puzzle, const emp_gm_config *config, emp_g
  *
  * Its device memory is one array of 4,232,448 bytes compiled into this
  * library, one copy per device. That is enough for every puzzle the library
- * accepts: up to 256 pieces and colour ids up to 31. Larger puzzles are
- * rejected with EMP_ERR_UNSUPPORTED and a message naming the limit.
+ * accepts: up to 256 pieces and colour ids up to 30 (emp_puzzle_create refuses
+ * higher ids). Larger puzzles are rejected with EMP_ERR_UNSUPPORTED and a
+ * message naming the limit.
  *
- * The first call on a device does a one-time set-up: it looks up the array's
- * device address, which loads the array onto the device. Make that first call
- * before any stream capture begins.
+ * The search runs on one block of one SM: config->blocks is ignored (the
+ * multi-block search of emp_glutton_max keeps its exchange buffers in
+ * allocated memory).
+ *
+ * Every call looks up the array's device address on the current device (this
+ * allocates nothing); the first call on a device also loads the array onto
+ * it. Make that first call before any stream capture begins.
  *
  * Every call shares the array, and the array keeps whatever the previous call
  * left. Each call rewrites everything the search reads before writing it.

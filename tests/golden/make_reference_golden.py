@@ -1,6 +1,6 @@
 """Extracts the reference's own golden vectors into tests/golden/reference_vectors.json.
 
-    python tests/golden/make_reference_golden.py [/path/to/reference]
+    python tests/golden/make_reference_golden.py /path/to/reference
 
 Reads, from the reference project (read-only):
   doc/example/{3_3,4_4,5_5,5_5_bis}.txt           example puzzles (CSV)
@@ -32,7 +32,9 @@ def expected_lines(path):
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_reference_golden.py /path/to/reference")
+    ref = sys.argv[1]
     data = {"source": "reference project tests and doc/example", "puzzles": {}, "new_strategy": {},
             "glutton_max": {}, "backtracker_first_solution": {}, "dump_solutions": {}}
     for name in ("3_3", "4_4", "5_5", "5_5_bis"):

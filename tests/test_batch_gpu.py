@@ -152,10 +152,19 @@ def test_full_batch_against_cpu_counts():
     handles = [native.NativePuzzle(p.width, p.height, p.colors) for p in batch]
     res = native.bt_count_batch(handles, split_subtrees=1024, timeout_ms=4000, use_graph=1, table_placement=1)
     checked = 0
+    golden7 = finished7 = 0
     for i, r in enumerate(res):
+        assert r.status in (native.EMP_OK, native.EMP_INCOMPLETE), (i, r.status)
         if r.status == native.EMP_OK and i in golden:
             assert (r.nodes, r.solutions) == golden[i], i
             checked += 1
         if i in golden and golden[i][0] < 20000 and batch[i].width <= 6:
             assert r.status == native.EMP_OK, i
+        if i in golden and batch[i].width == 7:
+            golden7 += 1
+            finished7 += r.status == native.EMP_OK
     assert checked >= 1500
+    # 7x7 instances wait behind other 7x7 subtrees, but most of the CPU-countable ones
+    # (trees below 1e9 placements) finish well inside the deadline; a scheduling change
+    # that starves them fails here
+    assert golden7 >= 100 and finished7 >= golden7 // 2, (finished7, golden7)
