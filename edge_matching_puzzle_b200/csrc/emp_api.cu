@@ -294,7 +294,7 @@ emp_status resume_records(const emp_puzzle_t& pz, const uint16_t* situation, uin
     std::vector<uint8_t> spilled(placed, 0);
     auto facing = [&](uint32_t e, uint32_t side) { return (e >> (5 * ((side + 2) & 3u))) & 31u; };
     for (uint32_t l = 0; l < placed; ++l) {
-        const uint32_t* d = &b[desc_off + 8 * l];
+        const uint32_t* d = &b[desc_off + emp::kDescWords * l];
         const uint32_t kw = d[0] & 0xFFu, nextra = (d[0] >> 13) & 7u, aoff = d[0] >> 16;
         const uint32_t ea = stk[d[1] & 0xFFu], eb = stk[(d[1] >> 8) & 0xFFu];
         const uint32_t row = d[2] + ((ea >> ((d[1] >> 16) & 0xFFu)) & 31u) * (d[3] & 0xFFFFu) +
@@ -427,14 +427,18 @@ emp_status create_plan(const emp_puzzle* puzzles, uint32_t count, const emp_bt_c
     cudaDeviceProp prop;
     CUDA_TRY(cudaGetDeviceProperties(&prop, pl->device));
     if (pl->max_kw > 32) return fail(EMP_ERR_UNSUPPORTED, "puzzle kinds wider than 32 candidate words");
+    if (pl->cfg.stack_placement > 3)
+        return fail(EMP_ERR_INVALID, "stack_placement must be 0 (default), 1, 2 or 3");
+    pl->stack_mode = pl->cfg.stack_placement ? static_cast<int>(pl->cfg.stack_placement) : emp::kStackShared16;
     std::vector<uint32_t> candidates;
     if (pl->cfg.threads_per_block) candidates.push_back(pl->cfg.threads_per_block);
     else candidates = {64, 128, 256, 512};
     int best_warps = 0;
     for (uint32_t threads : candidates) {
-        const void* fn = emp::dfs_kernel_symbol(pl->max_kw, pl->smem_tab_words != 0, threads);
+        const void* fn = emp::dfs_kernel_symbol(pl->max_kw, pl->smem_tab_words != 0, threads, pl->stack_mode);
         if (!fn) return fail(EMP_ERR_INVALID, "threads_per_block must be 64, 128, 256 or 512");
-        const size_t smem = emp::dfs_smem_bytes(pl->max_levels, pl->max_avail, threads, pl->smem_tab_words);
+        const size_t smem =
+            emp::dfs_smem_bytes(pl->max_levels, pl->max_avail, threads, pl->smem_tab_words, pl->stack_mode);
         if (smem > static_cast<size_t>(prop.sharedMemPerBlockOptin)) continue;
         CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
         int per_sm = 0;
@@ -451,6 +455,8 @@ emp_status create_plan(const emp_puzzle* puzzles, uint32_t count, const emp_bt_c
         return fail(EMP_ERR_UNSUPPORTED, "per-thread DFS state does not fit shared memory; use fewer threads per block");
     CUDA_TRY(pl->spill.alloc(sizeof(uint32_t) * static_cast<size_t>(pl->blocks) * pl->threads * pl->max_levels *
                              pl->max_kw));
+    if (pl->stack_mode == emp::kStackGlobal32)
+        CUDA_TRY(pl->stack.alloc(sizeof(uint32_t) * static_cast<size_t>(pl->blocks) * pl->threads * pl->max_levels));
     // round queues: room for every resident thread to hand back a full path twice
     const uint64_t resident = static_cast<uint64_t>(pl->blocks) * pl->threads;
     pl->capacity = std::max<uint64_t>(resident * 2 * (pl->max_levels - pl->depth + 1) / 4, 1u << 16);

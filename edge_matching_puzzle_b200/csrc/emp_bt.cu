@@ -222,13 +222,20 @@ __global__ void scan_apply(const uint32_t* __restrict__ in, uint64_t n, const ui
 // [3] puzzle | spilled<<16 | empty<<17, [4..] transitions (u16 pairs), then
 // the remaining set of level len (max_kw 32-bit words).
 //
-// Per-thread state in shared memory, thread-interleaved with a compile-time
-// block size T (a warp touching its own entries hits distinct banks and every
-// address is base + immediate):
-//   stk[L*T + tid] = more<<31 | t<<21 | spilled<<20 | colours of the placed piece
-//                    (more: candidates may remain after t; exact within t's word,
-//                    over-approximated by the row's occupancy beyond it)
-//   av[w*T + tid]  = 32-bit availability words of the three kinds
+// Per-thread state, thread-interleaved with a compile-time block size T (a warp
+// touching its own entries hits distinct banks and every address is base +
+// immediate):
+//   av[w*T + tid]  = 32-bit availability words of the three kinds (shared memory)
+//   the DFS stack, one entry per level, in one of three placements (StackMode):
+//     kStackShared32: shared memory, more<<31 | t<<21 | spilled<<20 | colours of
+//                     the placed piece (5 bits per side)
+//     kStackShared16: shared memory, more<<15 | spilled<<14 | t: half the bytes, so
+//                     more threads fit on an SM; a neighbour's colours are read from
+//                     the transition table of its kind instead
+//     kStackGlobal32: the 32-bit form in global memory (cached in L1), which leaves
+//                     shared memory to the tables and the availability words
+//   more: candidates may remain after t (exact within t's word, over-approximated
+//   by the row's occupancy beyond it).
 struct ThreadItem {
     uint64_t orig;
     const uint32_t* tb;
@@ -250,21 +257,68 @@ struct Tab;
 template <>
 struct Tab<true> {
     static __device__ __forceinline__ uint32_t u32(const ThreadItem&, uint32_t off) { return g_smem[off]; }
-    static __device__ __forceinline__ LevelDesc desc(const ThreadItem& s, uint32_t L)
+    static __device__ __forceinline__ LevelDesc desc(const ThreadItem& s, uint32_t L, bool ext)
     {
-        const uint4* d = reinterpret_cast<const uint4*>(g_smem + s.desc_off + 8 * L);
+        const uint4* d = reinterpret_cast<const uint4*>(g_smem + s.desc_off + kDescWords * L);
         const uint4 a = d[0], b = d[1];
-        return LevelDesc{a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+        const uint4 c = ext ? d[2] : make_uint4(0, 0, 0, 0);
+        return LevelDesc{a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w, c.x, c.y, c.z, c.w};
     }
 };
 
 template <>
 struct Tab<false> {
     static __device__ __forceinline__ uint32_t u32(const ThreadItem& s, uint32_t off) { return ldg(s.tb + off); }
-    static __device__ __forceinline__ LevelDesc desc(const ThreadItem& s, uint32_t L)
+    static __device__ __forceinline__ LevelDesc desc(const ThreadItem& s, uint32_t L, bool ext)
     {
-        return load_desc(s.tb, s.desc_off, L);
+        return load_desc(s.tb, s.desc_off, L, ext);
     }
+};
+
+// The thread's DFS stack (see above).  colour(): the colour that the piece placed
+// at level l shows at bit offset `shift` of its colour word (5 bits per side);
+// `tinfo` is the transition table of that level's kind (kStackShared16 only).
+template <int MODE, int T>
+struct Stk;
+
+template <int T>
+struct Stk<kStackShared32, T> {
+    uint32_t* p;
+    __device__ __forceinline__ uint32_t t(uint32_t l) const { return (p[l * T] >> 21) & 0x3FFu; }
+    __device__ __forceinline__ bool more(uint32_t l) const { return (p[l * T] >> 31) != 0; }
+    __device__ __forceinline__ uint32_t spilled(uint32_t l) const { return (p[l * T] >> 20) & 1u; }
+    __device__ __forceinline__ void put(uint32_t l, uint32_t t, bool more, uint32_t spilled, uint32_t ti)
+    {
+        p[l * T] = (static_cast<uint32_t>(more) << 31) | (t << 21) | (spilled << 20) | (ti & 0xFFFFFu);
+    }
+    template <bool SM>
+    __device__ __forceinline__ uint32_t colour(const ThreadItem&, uint32_t l, uint32_t shift, uint32_t) const
+    {
+        return (p[l * T] >> shift) & 31u;
+    }
+    static constexpr bool kNeedsKindTables = false;
+};
+
+template <int T>
+struct Stk<kStackGlobal32, T> : Stk<kStackShared32, T> {
+};
+
+template <int T>
+struct Stk<kStackShared16, T> {
+    uint16_t* p;
+    __device__ __forceinline__ uint32_t t(uint32_t l) const { return p[l * T] & 0x3FFu; }
+    __device__ __forceinline__ bool more(uint32_t l) const { return (p[l * T] >> 15) != 0; }
+    __device__ __forceinline__ uint32_t spilled(uint32_t l) const { return (p[l * T] >> 14) & 1u; }
+    __device__ __forceinline__ void put(uint32_t l, uint32_t t, bool more, uint32_t spilled, uint32_t)
+    {
+        p[l * T] = static_cast<uint16_t>((static_cast<uint32_t>(more) << 15) | (spilled << 14) | t);
+    }
+    template <bool SM>
+    __device__ __forceinline__ uint32_t colour(const ThreadItem& s, uint32_t l, uint32_t shift, uint32_t tinfo) const
+    {
+        return (Tab<SM>::u32(s, tinfo + t(l)) >> shift) & 31u;
+    }
+    static constexpr bool kNeedsKindTables = true;
 };
 
 __device__ __forceinline__ uint32_t rec_t(const uint32_t* rec, uint32_t l)
@@ -272,8 +326,8 @@ __device__ __forceinline__ uint32_t rec_t(const uint32_t* rec, uint32_t l)
     return (rec[4 + (l >> 1)] >> (16 * (l & 1))) & 0xFFFFu;
 }
 
-template <bool SM, int T>
-__device__ __forceinline__ void load_record(const BtLaunch& P, ThreadItem& s, const uint32_t* rec, uint32_t* stk,
+template <bool SM, int T, class S>
+__device__ __forceinline__ void load_record(const BtLaunch& P, ThreadItem& s, const uint32_t* rec, S& stk,
                                             uint32_t* av, uint32_t* spill)
 {
     using TB = Tab<SM>;
@@ -288,10 +342,11 @@ __device__ __forceinline__ void load_record(const BtLaunch& P, ThreadItem& s, co
     const uint32_t aw = TB::u32(s, H_AWORDS), init = TB::u32(s, H_INIT);
     for (uint32_t w = 0; w < aw; ++w) av[w * T] = ldg(s.tb + init + w);
     for (uint32_t l = 0; l < len; ++l) {
-        const uint32_t d0 = TB::u32(s, s.desc_off + 8 * l), d5 = TB::u32(s, s.desc_off + 8 * l + 5);
+        const uint32_t d0 = TB::u32(s, s.desc_off + kDescWords * l);
+        const uint32_t d5 = TB::u32(s, s.desc_off + kDescWords * l + 5);
         const uint32_t t = rec_t(rec, l);
         av[((d0 >> 16) + (t >> 5)) * T] &= ~(0xFu << (t & 28u));
-        stk[l * T] = (t << 21) | (TB::u32(s, d5 + t) & 0xFFFFFu);
+        stk.put(l, t, false, 0u, S::kNeedsKindTables ? 0u : TB::u32(s, d5 + t));
     }
     if (s.spilled) {
         const uint32_t* R = rec + P.rec_r_off;
@@ -306,19 +361,29 @@ __device__ __forceinline__ void load_record(const BtLaunch& P, ThreadItem& s, co
     s.active = true;
 }
 
+// Pair-table row of level L: its first two placed neighbours' facing colours
+// index it (a neighbour that is absent has stride 0).
+template <bool SM, class S>
+__device__ __forceinline__ uint32_t level_row(const ThreadItem& s, const LevelDesc& d, const S& stk)
+{
+    const uint32_t ca = stk.template colour<SM>(s, d.level_a(), d.shift_a(), d.d8);
+    const uint32_t cb = stk.template colour<SM>(s, d.level_b(), d.shift_b(), d.d9);
+    return d.d2 + ca * d.stride_a() + cb * d.stride_b();
+}
+
 // Candidate word w of level L from its pair-table row (frame sides & the first
 // two placed neighbours), the availability, and the side masks of further placed
 // neighbours (never present in row-major order).
-template <bool SM, int T>
+template <bool SM, int T, class S>
 __device__ __forceinline__ uint32_t candidate_word(const ThreadItem& s, const LevelDesc& d, uint32_t row, uint32_t w,
-                                                   const uint32_t* stk, const uint32_t* av)
+                                                   const S& stk, const uint32_t* av)
 {
     uint32_t x = Tab<SM>::u32(s, row + 1 + w) & av[(d.aoff() + w) * T];
     if (d.nextra()) {
         const uint32_t ncol = Tab<SM>::u32(s, H_NCOL), kw = d.kw();
         for (uint32_t j = 0; j < d.nextra(); ++j) {
             const uint32_t sd = d.extra_side(j);
-            const uint32_t c = facing_colour(stk[d.extra_level(j) * T], sd);
+            const uint32_t c = stk.template colour<SM>(s, d.extra_level(j), 5 * ((sd + 2) & 3u), j ? d.d11 : d.d10);
             x &= ldg(s.tb + d.d4 + (sd * ncol + c) * kw + w);
         }
     }
@@ -328,9 +393,9 @@ __device__ __forceinline__ uint32_t candidate_word(const ThreadItem& s, const Le
 // First candidate t >= start of level L, and whether more may follow it.  The
 // unspilled walk visits only the row's occupied words; `more` is exact within
 // t's word and counts any later occupied row word.  Returns false when none.
-template <bool SM, int T>
+template <bool SM, int T, class S>
 __device__ __forceinline__ bool find_candidate(const BtLaunch& P, const ThreadItem& s, const LevelDesc& d, uint32_t L,
-                                               uint32_t start, bool spilled, const uint32_t* stk, const uint32_t* av,
+                                               uint32_t start, bool spilled, const S& stk, const uint32_t* av,
                                                const uint32_t* spill, uint32_t* t_out, bool* more_out)
 {
     const uint32_t sw = start >> 5;
@@ -351,7 +416,7 @@ __device__ __forceinline__ bool find_candidate(const BtLaunch& P, const ThreadIt
         }
         return false;
     }
-    const uint32_t row = d.row(stk[d.level_a() * T], stk[d.level_b() * T]);
+    const uint32_t row = level_row<SM>(s, d, stk);
     uint32_t occ = Tab<SM>::u32(s, row) & shl32(~0u, sw);
     while (occ) {
         const uint32_t w = __ffs(occ) - 1;
@@ -368,15 +433,14 @@ __device__ __forceinline__ bool find_candidate(const BtLaunch& P, const ThreadIt
 }
 
 // Goes up one level: gives back the piece placed there and resumes after it.
-template <bool SM, int T>
-__device__ __forceinline__ void pop_level(ThreadItem& s, const uint32_t* stk, uint32_t* av)
+template <bool SM, int T, class S>
+__device__ __forceinline__ void pop_level(ThreadItem& s, const S& stk, uint32_t* av)
 {
     --s.L;
-    const uint32_t e = stk[s.L * T];
-    const uint32_t t = (e >> 21) & 0x3FFu;
-    s.spilled = (e >> 20) & 1u;
-    s.pop = !(e >> 31);
-    const uint32_t aoff = Tab<SM>::u32(s, s.desc_off + 8 * s.L) >> 16;
+    const uint32_t t = stk.t(s.L);
+    s.spilled = stk.spilled(s.L);
+    s.pop = !stk.more(s.L);
+    const uint32_t aoff = Tab<SM>::u32(s, s.desc_off + kDescWords * s.L) >> 16;
     av[(aoff + (t >> 5)) * T] |= 0xFu << (t & 28u);
     s.start = t + 1;
 }
@@ -386,16 +450,16 @@ __device__ __forceinline__ void pop_level(ThreadItem& s, const uint32_t* stk, ui
 // place the next candidate of the current level, or go up one level when it has
 // none.  Doing the known pops and the next try in the same step keeps the lanes
 // of a warp on the same (try) path.  Returns false once the record is exhausted.
-template <bool SM, int T>
-__device__ __forceinline__ bool dfs_step(const BtLaunch& P, ThreadItem& s, uint32_t* stk, uint32_t* av,
-                                         uint32_t* spill, bool* solved)
+template <bool SM, int T, class S>
+__device__ __forceinline__ bool dfs_step(const BtLaunch& P, ThreadItem& s, S& stk, uint32_t* av, uint32_t* spill,
+                                         bool* solved)
 {
     while (s.pop) {
         if (s.L == s.base) return false;
         pop_level<SM, T>(s, stk, av);
     }
     {
-        const LevelDesc d = Tab<SM>::desc(s, s.L);
+        const LevelDesc d = Tab<SM>::desc(s, s.L, S::kNeedsKindTables);
         uint32_t t;
         bool more;
         if (find_candidate<SM, T>(P, s, d, s.L, s.start, s.spilled != 0, stk, av, spill, &t, &more)) {
@@ -407,7 +471,7 @@ __device__ __forceinline__ bool dfs_step(const BtLaunch& P, ThreadItem& s, uint3
                 const uint32_t kw = d.kw();
                 uint32_t* sp = spill + s.L * P.max_kw;
                 const uint32_t* ex = s.tb + d.d6 + t * kw;
-                const uint32_t row = s.spilled ? 0u : d.row(stk[d.level_a() * T], stk[d.level_b() * T]);
+                const uint32_t row = s.spilled ? 0u : level_row<SM>(s, d, stk);
                 const uint32_t tw = t >> 5;
                 bool rest = false;
                 for (uint32_t w = 0; w < kw; ++w) {
@@ -423,7 +487,7 @@ __device__ __forceinline__ bool dfs_step(const BtLaunch& P, ThreadItem& s, uint3
             uint32_t& aw = av[(d.aoff() + (t >> 5)) * T];
             const uint32_t nib = 0xFu << (t & 28u);
             aw &= ~nib;
-            stk[s.L * T] = (static_cast<uint32_t>(more) << 31) | (t << 21) | (s.spilled << 20) | (ti & 0xFFFFFu);
+            stk.put(s.L, t, more, s.spilled, ti);
             ++s.nodes;
             if (s.L == s.n - 1) {
                 // solution: count it, give the piece back, try the next candidate
@@ -451,8 +515,8 @@ __device__ __forceinline__ bool dfs_step(const BtLaunch& P, ThreadItem& s, uint3
 // its first solution.  The lock is held for a few hundred cycles; the wait for
 // it is bounded in time (first_lock_wait_ns of %globaltimer) and a thread that
 // gives up flags the record as missed, which the host reports as EMP_FIRST_LOST.
-template <int T>
-__device__ void record_solution(const BtLaunch& P, const ThreadItem& s, const uint32_t* stk)
+template <class S>
+__device__ void record_solution(const BtLaunch& P, const ThreadItem& s, const S& stk)
 {
     FirstRecord* r = P.first_records + s.pz;
     atomicMin(&P.first_item[s.pz], (unsigned long long)s.orig);
@@ -470,7 +534,7 @@ __device__ void record_solution(const BtLaunch& P, const ThreadItem& s, const ui
     bool better = !r->has;
     if (!better) {
         for (uint32_t l = 0; l < s.n; ++l) {
-            const uint32_t mine = (stk[l * T] >> 21) & 0x3FFu, theirs = r->t[l];
+            const uint32_t mine = stk.t(l), theirs = r->t[l];
             if (mine != theirs) {
                 better = mine < theirs;
                 break;
@@ -478,7 +542,7 @@ __device__ void record_solution(const BtLaunch& P, const ThreadItem& s, const ui
         }
     }
     if (better) {
-        for (uint32_t l = 0; l < s.n; ++l) r->t[l] = static_cast<uint16_t>((stk[l * T] >> 21) & 0x3FFu);
+        for (uint32_t l = 0; l < s.n; ++l) r->t[l] = static_cast<uint16_t>(stk.t(l));
         r->has = 1;
     }
     __threadfence();
@@ -498,8 +562,8 @@ __device__ __forceinline__ void account(const BtLaunch& P, const ThreadItem& s)
 // Remaining candidates of level l (current level: from s.start unless it is
 // known exhausted; shallower levels: after their placed transition, when the
 // `more` bit says some may remain), with `av` holding level l's entry availability.
-template <bool SM, int T>
-__device__ __forceinline__ bool level_has_work(const BtLaunch& P, const ThreadItem& s, uint32_t l, const uint32_t* stk,
+template <bool SM, int T, class S>
+__device__ __forceinline__ bool level_has_work(const BtLaunch& P, const ThreadItem& s, uint32_t l, const S& stk,
                                                const uint32_t* av, const uint32_t* spill, uint32_t* start_out,
                                                uint32_t* spilled_out)
 {
@@ -510,26 +574,25 @@ __device__ __forceinline__ bool level_has_work(const BtLaunch& P, const ThreadIt
         spilled = s.spilled;
         maybe = !s.pop;
     } else {
-        const uint32_t e = stk[l * T];
-        start = ((e >> 21) & 0x3FFu) + 1;
-        spilled = (e >> 20) & 1u;
-        maybe = (e >> 31) != 0;
+        start = stk.t(l) + 1;
+        spilled = stk.spilled(l);
+        maybe = stk.more(l);
     }
     *start_out = start;
     *spilled_out = spilled;
     if (!maybe) return false;
-    const LevelDesc d = Tab<SM>::desc(s, l);
+    const LevelDesc d = Tab<SM>::desc(s, l, S::kNeedsKindTables);
     uint32_t t;
     bool more;
     return find_candidate<SM, T>(P, s, d, l, start, spilled != 0, stk, av, spill, &t, &more);
 }
 
-template <bool SM, int T>
-__device__ __forceinline__ void toggle_piece(const ThreadItem& s, uint32_t l, const uint32_t* stk, uint32_t* av,
+template <bool SM, int T, class S>
+__device__ __forceinline__ void toggle_piece(const ThreadItem& s, uint32_t l, const S& stk, uint32_t* av,
                                              bool give_back)
 {
-    const uint32_t aoff = Tab<SM>::u32(s, s.desc_off + 8 * l) >> 16;
-    const uint32_t t = (stk[l * T] >> 21) & 0x3FFu;
+    const uint32_t aoff = Tab<SM>::u32(s, s.desc_off + kDescWords * l) >> 16;
+    const uint32_t t = stk.t(l);
     if (give_back) av[(aoff + (t >> 5)) * T] |= 0xFu << (t & 28u);
     else av[(aoff + (t >> 5)) * T] &= ~(0xFu << (t & 28u));
 }
@@ -540,8 +603,8 @@ __device__ __forceinline__ void toggle_piece(const ThreadItem& s, uint32_t l, co
 // availability, and counts; pass 2 walks back down, writing records and taking
 // the pieces again, which leaves the state as it was.  Returns false when the
 // output queue is full (the thread then keeps the work).
-template <bool SM, int T>
-__device__ bool split_record(const BtLaunch& P, ThreadItem& s, uint32_t* stk, uint32_t* av, const uint32_t* spill)
+template <bool SM, int T, class S>
+__device__ bool split_record(const BtLaunch& P, ThreadItem& s, const S& stk, uint32_t* av, const uint32_t* spill)
 {
     uint32_t cnt = 0, start, spilled;
     for (uint32_t l = s.L + 1; l-- > s.base;) {
@@ -560,8 +623,8 @@ __device__ bool split_record(const BtLaunch& P, ThreadItem& s, uint32_t* stk, ui
                 rec[2] = l | (start << 16);
                 rec[3] = s.pz | (spilled << 16);
                 for (uint32_t j = 0; j < l; j += 2) {
-                    const uint32_t lo = (stk[j * T] >> 21) & 0x3FFu;
-                    const uint32_t hi = j + 1 < l ? (stk[(j + 1) * T] >> 21) & 0x3FFu : 0u;
+                    const uint32_t lo = stk.t(j);
+                    const uint32_t hi = j + 1 < l ? stk.t(j + 1) : 0u;
                     rec[4 + (j >> 1)] = lo | (hi << 16);
                 }
                 if (spilled)
@@ -576,7 +639,7 @@ __device__ bool split_record(const BtLaunch& P, ThreadItem& s, uint32_t* stk, ui
     return fits;
 }
 
-template <bool SM, int T, int kStepsPerFetch>
+template <bool SM, int T, int MODE, int kStepsPerFetch>
 __global__ void __launch_bounds__(T) dfs_kernel(BtLaunch P)
 {
     const uint32_t tid = threadIdx.x, lane = tid & 31;
@@ -587,9 +650,18 @@ __global__ void __launch_bounds__(T) dfs_kernel(BtLaunch P)
         for (uint32_t i = tid; i < P.smem_tab_words / 4; i += T) dst[i] = __ldg(src + i);
         __syncthreads();
     }
-    // this thread's columns of the interleaved state
-    uint32_t* stk = g_smem + P.smem_tab_words + tid;
-    uint32_t* av = g_smem + P.smem_tab_words + P.max_levels * T + tid;
+    // this thread's columns of the interleaved state: availability words, then
+    // (shared placements) the stack
+    uint32_t* av = g_smem + P.smem_tab_words + tid;
+    Stk<MODE, T> stk;
+    if (MODE == kStackGlobal32) {
+        *reinterpret_cast<uint32_t**>(&stk.p) = P.stack + (size_t)blockIdx.x * T * P.max_levels + tid;
+    } else if (MODE == kStackShared32) {
+        *reinterpret_cast<uint32_t**>(&stk.p) = g_smem + P.smem_tab_words + P.max_avail_words * T + tid;
+    } else {
+        *reinterpret_cast<uint16_t**>(&stk.p) =
+            reinterpret_cast<uint16_t*>(g_smem + P.smem_tab_words + P.max_avail_words * T) + tid;
+    }
     uint32_t* spill = P.spill + (size_t)(blockIdx.x * T + tid) * P.max_levels * P.max_kw;
     ThreadItem s;
     s.active = false;
@@ -646,7 +718,7 @@ __global__ void __launch_bounds__(T) dfs_kernel(BtLaunch P)
                 bool solved = false;
                 if (dfs_step<SM, T>(P, s, stk, av, spill, &solved)) {
                     if (solved) {
-                        record_solution<T>(P, s, stk);
+                        record_solution(P, s, stk);
                         if (P.sols) {
                             const unsigned long long slot = atomicAdd(P.sol_count, 1ull);
                             if (slot < P.sol_capacity) {
@@ -654,7 +726,7 @@ __global__ void __launch_bounds__(T) dfs_kernel(BtLaunch P)
                                 r->orig = s.orig;
                                 r->local = s.nodes;
                                 for (uint32_t l = 0; l < s.n; ++l)
-                                    r->t[l] = static_cast<uint16_t>((stk[l * T] >> 21) & 0x3FFu);
+                                    r->t[l] = static_cast<uint16_t>(stk.t(l));
                             }
                         }
                         if (P.stop_at_any) {
@@ -835,21 +907,32 @@ __global__ void record_prefix(const uint32_t* __restrict__ rec, uint32_t rec_wor
     for (uint32_t l = threadIdx.x; l < 256; l += blockDim.x) out[l] = l < len ? static_cast<uint16_t>(rec_t(r, l)) : 0xFFFFu;
 }
 
-template <int T>
+template <int T, int MODE>
 const void* dfs_symbol(bool sm)
 {
-    return sm ? reinterpret_cast<const void*>(&dfs_kernel<true, T, 32>)
-              : reinterpret_cast<const void*>(&dfs_kernel<false, T, 32>);
+    return sm ? reinterpret_cast<const void*>(&dfs_kernel<true, T, MODE, 32>)
+              : reinterpret_cast<const void*>(&dfs_kernel<false, T, MODE, 32>);
 }
 
-const void* dfs_symbol_for(uint32_t max_kw, bool sm, uint32_t threads)
+template <int T>
+const void* dfs_symbol_mode(bool sm, int mode)
+{
+    switch (mode) {
+        case kStackShared32: return dfs_symbol<T, kStackShared32>(sm);
+        case kStackShared16: return dfs_symbol<T, kStackShared16>(sm);
+        case kStackGlobal32: return dfs_symbol<T, kStackGlobal32>(sm);
+        default: return nullptr;
+    }
+}
+
+const void* dfs_symbol_for(uint32_t max_kw, bool sm, uint32_t threads, int mode)
 {
     if (max_kw > kMaxKindWords) return nullptr;
     switch (threads) {
-        case 64: return dfs_symbol<64>(sm);
-        case 128: return dfs_symbol<128>(sm);
-        case 256: return dfs_symbol<256>(sm);
-        case 512: return dfs_symbol<512>(sm);
+        case 64: return dfs_symbol_mode<64>(sm, mode);
+        case 128: return dfs_symbol_mode<128>(sm, mode);
+        case 256: return dfs_symbol_mode<256>(sm, mode);
+        case 512: return dfs_symbol_mode<512>(sm, mode);
         default: return nullptr;
     }
 }
@@ -916,24 +999,27 @@ cudaError_t launch_scan(const uint32_t* counts, uint64_t n, uint64_t* offsets, u
 
 uint64_t scan_block_sum_words(uint64_t n) { return (n + kScanBlock - 1) / kScanBlock + 1; }
 
-size_t dfs_smem_bytes(uint32_t max_levels, uint32_t max_avail_words, uint32_t threads, uint32_t tab_words)
+size_t dfs_smem_bytes(uint32_t max_levels, uint32_t max_avail_words, uint32_t threads, uint32_t tab_words,
+                      int stack_mode)
 {
+    const size_t stack = stack_mode == kStackShared32 ? 4 : (stack_mode == kStackShared16 ? 2 : 0);
     return static_cast<size_t>(tab_words) * sizeof(uint32_t) +
-           (static_cast<size_t>(max_levels) + static_cast<size_t>(max_avail_words)) * sizeof(uint32_t) * threads;
+           static_cast<size_t>(max_avail_words) * sizeof(uint32_t) * threads +
+           ((static_cast<size_t>(max_levels) * stack * threads + 3) & ~size_t(3));
 }
 
 uint32_t record_words(uint32_t max_levels, uint32_t max_kw) { return 4 + (max_levels + 1) / 2 + max_kw; }
 
-const void* dfs_kernel_symbol(uint32_t max_kw, bool smem_tables, uint32_t threads)
+const void* dfs_kernel_symbol(uint32_t max_kw, bool smem_tables, uint32_t threads, int stack_mode)
 {
-    return dfs_symbol_for(max_kw, smem_tables, threads);
+    return dfs_symbol_for(max_kw, smem_tables, threads, stack_mode);
 }
 
 cudaError_t launch_dfs(const BtLaunch& P, uint32_t blocks, uint32_t threads, cudaStream_t stream)
 {
-    const void* fn = dfs_symbol_for(P.max_kw, P.smem_tab_words != 0, threads);
+    const void* fn = dfs_symbol_for(P.max_kw, P.smem_tab_words != 0, threads, P.stack_mode);
     if (!fn) return cudaErrorInvalidValue;
-    const size_t smem = dfs_smem_bytes(P.max_levels, P.max_avail_words, threads, P.smem_tab_words);
+    const size_t smem = dfs_smem_bytes(P.max_levels, P.max_avail_words, threads, P.smem_tab_words, P.stack_mode);
     void* args[] = {const_cast<BtLaunch*>(&P)};
     return cudaLaunchKernel(fn, dim3(blocks), dim3(threads), args, smem, stream);
 }

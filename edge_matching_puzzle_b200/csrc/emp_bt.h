@@ -1,6 +1,8 @@
 // Launch interface of the exhaustive backtracker kernels (emp_bt.cu).
 #pragma once
 
+#include "emp_layout.h"
+
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -83,6 +85,8 @@ struct BtLaunch {
     unsigned long long sol_capacity = 0;
     unsigned long long first_lock_wait_ns = 20000000ull;  // bound of a wait for a first-solution record
     uint32_t first_lock_init = 0;             // value the records' locks start at (1: held by nobody; tests)
+    int stack_mode = kStackShared32;          // placement of the per-thread DFS stack (StackMode)
+    uint32_t* stack = nullptr;                // kStackGlobal32: [blocks][max_levels][threads] stack entries
 };
 
 cudaError_t launch_expand(const BtLaunch& P, const uint16_t* parents, const uint32_t* parent_puzzle,
@@ -92,7 +96,8 @@ cudaError_t launch_expand(const BtLaunch& P, const uint16_t* parents, const uint
 cudaError_t launch_scan(const uint32_t* counts, uint64_t n, uint64_t* offsets, uint64_t* block_sums,
                         uint64_t* grand_total, cudaStream_t stream);
 uint64_t scan_block_sum_words(uint64_t n);
-size_t dfs_smem_bytes(uint32_t max_levels, uint32_t max_avail_words, uint32_t threads, uint32_t tab_words);
+size_t dfs_smem_bytes(uint32_t max_levels, uint32_t max_avail_words, uint32_t threads, uint32_t tab_words,
+                      int stack_mode);
 uint32_t record_words(uint32_t max_levels, uint32_t max_kw);
 cudaError_t launch_dfs(const BtLaunch& P, uint32_t blocks, uint32_t threads, cudaStream_t stream);
 cudaError_t launch_bt_reset(const BtLaunch& P, uint32_t n_puzzles, cudaStream_t stream);
@@ -124,6 +129,6 @@ cudaError_t launch_solution_index(const SolutionRecord* sols, uint64_t nsol, con
                                   unsigned long long* out, cudaStream_t stream);
 cudaError_t launch_record_prefix(const uint32_t* rec, uint32_t rec_words, uint64_t i, uint16_t* out,
                                  cudaStream_t stream);
-const void* dfs_kernel_symbol(uint32_t max_kw, bool smem_tables, uint32_t threads);
+const void* dfs_kernel_symbol(uint32_t max_kw, bool smem_tables, uint32_t threads, int stack_mode);
 
 }  // namespace emp

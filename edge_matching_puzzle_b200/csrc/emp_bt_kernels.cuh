@@ -13,6 +13,8 @@
 // kind_index*4 + orientation lives in 32-bit word t>>5, bit t&31.
 #pragma once
 
+#include "emp_layout.h"
+
 #include <cstdint>
 
 namespace emp {
@@ -28,6 +30,8 @@ __device__ __forceinline__ uint32_t ldg(const uint32_t* p) { return __ldg(p); }
 
 struct LevelDesc {
     uint32_t d0, d1, d2, d3, d4, d5, d6, d7;
+    // transition tables of the kinds of neighbours A, B and the extra ones (read when asked for)
+    uint32_t d8 = 0, d9 = 0, d10 = 0, d11 = 0;
     __device__ __forceinline__ uint32_t kw() const { return d0 & 0xFFu; }
     __device__ __forceinline__ uint32_t kind() const { return (d0 >> 8) & 3u; }
     __device__ __forceinline__ uint32_t nextra() const { return (d0 >> 13) & 7u; }
@@ -48,11 +52,12 @@ struct LevelDesc {
     }
 };
 
-__device__ __forceinline__ LevelDesc load_desc(const uint32_t* tb, uint32_t desc_off, uint32_t L)
+__device__ __forceinline__ LevelDesc load_desc(const uint32_t* tb, uint32_t desc_off, uint32_t L, bool ext = false)
 {
-    const uint4* d = reinterpret_cast<const uint4*>(tb + desc_off + 8 * L);
+    const uint4* d = reinterpret_cast<const uint4*>(tb + desc_off + kDescWords * L);
     const uint4 a = __ldg(d), b = __ldg(d + 1);
-    return LevelDesc{a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+    const uint4 c = ext ? __ldg(d + 2) : make_uint4(0, 0, 0, 0);
+    return LevelDesc{a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w, c.x, c.y, c.z, c.w};
 }
 
 // colour that the neighbour placed at the level whose stack word is `e`

@@ -306,7 +306,7 @@ void build_device_tables(const PuzzleModel& m, const std::vector<LevelPlan>& pla
     // level descriptors
     align(b, 4);
     t.desc_off = static_cast<uint32_t>(b.size());
-    b.resize(b.size() + 8 * static_cast<size_t>(m.n), 0);
+    b.resize(b.size() + kDescWords * static_cast<size_t>(m.n), 0);
     // transition info
     for (uint32_t k = 0; k < 3; ++k) {
         t.tinfo_off[k] = static_cast<uint32_t>(b.size());
@@ -354,7 +354,7 @@ void build_device_tables(const PuzzleModel& m, const std::vector<LevelPlan>& pla
     align(b, 4);
     for (uint32_t L = 0; L < m.n; ++L) {
         const LevelPlan& lp = plan[L];
-        uint32_t* d = &b[t.desc_off + 8 * L];
+        uint32_t* d = &b[t.desc_off + kDescWords * L];
         const uint32_t k = lp.kind;
         const uint32_t arity = std::min<uint32_t>(lp.nplaced, 2);
         const uint32_t nextra = lp.nplaced - arity;
@@ -374,6 +374,10 @@ void build_device_tables(const PuzzleModel& m, const std::vector<LevelPlan>& pla
         d[6] = t.extra_off[k];
         d[7] = (nextra > 0 ? lp.side[2] : 0u) | ((nextra > 1 ? lp.side[3] : 0u) << 2) |
                ((nextra > 0 ? lp.nb_level[2] : 0u) << 8) | ((nextra > 1 ? lp.nb_level[3] : 0u) << 16);
+        for (uint32_t j = 0; j < 4; ++j) {
+            const uint32_t lev = j < lp.nplaced ? lp.nb_level[j] : 0u;
+            d[8 + j] = t.tinfo_off[plan[lev].kind];
+        }
     }
     b[0] = 0x454D5033u;  // "EMP3": 32-bit candidate words
     b[1] = t.n;

@@ -25,6 +25,8 @@
 // the device tables alike.
 #pragma once
 
+#include "emp_layout.h"
+
 #include <array>
 #include <cstdint>
 #include <string>
@@ -87,8 +89,8 @@ struct LevelPlan {
 //   23 height, 24 blob words, 25 max kw, 26 words of the hot prefix
 // sections in order: header, pair tables, desc, tinfo, side, extra, initial
 // availability; the hot prefix [0, side[0]) is what the DFS reads at every step
-// desc (8 words per level; the first two placed neighbours A and B index the
-// level's pair table, further placed neighbours AND their side masks):
+// desc (kDescWords = 16 words per level; the first two placed neighbours A and B
+// index the level's pair table, further placed neighbours AND their side masks):
 //   d0 kw | kind<<8 | nextra<<13 | aoff<<16
 //   d1 levelA | levelB<<8 | shiftA<<16 | shiftB<<24 (bit offset of the
 //      neighbour's facing colour in its stack word)
@@ -98,6 +100,9 @@ struct LevelPlan {
 //   d3 strideA | strideB<<16 (words per colour step of A and B; 0 when absent)
 //   d4 side[kind], d5 tinfo[kind], d6 extra[kind],
 //   d7 extra placed sides: side3 | side4<<2 | level3<<8 | level4<<16
+//   d8..d11 tinfo[kind] of the levels of neighbours A, B, 3 and 4 (level 0's kind
+//      when absent), for a stack that keeps transitions without their colours
+//   d12..d15 0
 // side[k]: [side][colour][kw[k]] masks (colour ncol-1 = frame)
 // tinfo[k]: per transition t, colours of the oriented piece (5 bits per side)
 //           | has_extra<<20 (its identical mask clears other candidates)

@@ -24,6 +24,8 @@ struct emp_bt_plan_t {
     DeviceBuffer rec_init, rec_a, rec_b;      // initial records (selection), round queues
     DeviceBuffer counters;                    // [0] cursor, [1] output tail
     DeviceBuffer totals, first_item, records, flags, item_nodes, item_sols, spill, prefix_out;
+    DeviceBuffer stack;                       // kStackGlobal32: the threads' DFS stacks
+    int stack_mode = emp::kStackShared16;
     DeviceBuffer ctl, incomplete, puzzle_depth_dev;
     std::vector<uint32_t> puzzle_depth;       // per puzzle split depth
     bool adaptive = false;                    // per puzzle split depths (split_subtrees)
@@ -107,6 +109,8 @@ struct emp_bt_plan_t {
         P.incomplete = incomplete.as<uint32_t>();
         if (cfg.first_lock_wait_us) P.first_lock_wait_ns = 1000ull * cfg.first_lock_wait_us;
         P.first_lock_init = cfg.hold_first_lock ? 1u : 0u;
+        P.stack_mode = stack_mode;
+        P.stack = stack.as<uint32_t>();
         return P;
     }
 };

@@ -68,7 +68,13 @@ extern "C" emp_status emp_bt_autotune(const emp_puzzle* puzzles, uint32_t count,
             best = cand;
         }
     };
-    for (uint32_t threads : {64u, 128u, 256u}) {
+    for (uint32_t placement : {1u, 2u, 3u}) {  // the DFS stack: shared 32-bit, shared 16-bit, global
+        if (placement == (best.stack_placement ? best.stack_placement : 2u)) continue;
+        emp_bt_config c = best;
+        c.stack_placement = placement;
+        consider(c);
+    }
+    for (uint32_t threads : {64u, 128u, 256u, 512u}) {
         if (threads == best.threads_per_block) continue;
         emp_bt_config c = best;
         c.threads_per_block = threads;

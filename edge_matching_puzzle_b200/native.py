@@ -61,6 +61,7 @@ class BtConfig(ctypes.Structure):
         ("stop_at_any", ctypes.c_uint32),
         ("first_lock_wait_us", ctypes.c_uint32),
         ("hold_first_lock", ctypes.c_uint32),
+        ("stack_placement", ctypes.c_uint32),
     ]
 
 

@@ -130,6 +130,11 @@ typedef struct emp_bt_config {
                                     A wait that runs out reports EMP_FIRST_LOST for the puzzle */
     uint32_t hold_first_lock;    /* testing only: 1 = every first-solution record starts locked by
                                     nobody, so each wait runs out (exercises EMP_FIRST_LOST) */
+    uint32_t stack_placement;    /* where each thread keeps its DFS stack: 0 = default (2),
+                                    1 = shared memory, 32-bit entries with the placed piece's colours,
+                                    2 = shared memory, 16-bit entries (more threads per SM; colours are
+                                        read from the transition table),
+                                    3 = global memory (L1-cached), 32-bit entries */
 } emp_bt_config;
 
 typedef struct emp_bt_result {
@@ -236,6 +241,7 @@ typedef struct emp_bt_tune_result {
 /* Chooses the launch parameters for a set of puzzles by timing short runs on the
  * device.  Starting from base (NULL = defaults), it tunes one field at a time, keeping
  * each field's fastest value before moving on:
+ *   stack_placement     the DFS stack in shared memory (32- or 16-bit entries) or global memory
  *   threads_per_block   64, 128, 256, 512
  *   split_subtrees      per-puzzle split targets (batches of several puzzles) or
  *   split_depth         split depths (a single puzzle)

@@ -96,3 +96,25 @@ def test_placement_budget_stops_the_search():
     assert st == native.EMP_INCOMPLETE and r.status == 1
     assert r.trials + r.pushes >= budget
     assert r.levels < full.levels
+
+
+def test_16x16_first_pushes_against_oracle():
+    """The 16x16 workload puzzle (5 border / 17 interior colours, seed 7) at its own size:
+    the first pushes of the GPU search, one block and the whole grid, take the oracle's
+    trajectory (tests/golden/glutton_16x16.json, made by make_glutton_counts.py: the
+    oracle needs minutes per push at this size)."""
+    import json
+    import os
+    with open(os.path.join(os.path.dirname(__file__), "golden", "glutton_16x16.json")) as f:
+        recs = json.load(f)["records"]
+    pz = generate(16, 16, 5, 17, 7)
+    h = native.NativePuzzle(16, 16, pz.colors)
+    for rec in recs:
+        for blocks in (1, 0):
+            got = native.glutton_max(h, push_budget=rec["push_budget"], timeout_ms=120000, blocks=blocks)
+            assert (got.status, got.max_level, got.level, got.pushes, got.pops, got.levels) == \
+                (rec["status"], rec["max_level"], rec["level"], rec["pushes"], rec["pops"], rec["levels_evaluated"])
+            cells = [-1] * 256
+            for pi in rec["played"]:
+                cells[pi & 0xFF] = (((pi >> 8) & 0xFF) << 2) | (pi >> 16)
+            assert [c if c != 0xFFFFFFFF else -1 for c in list(got.final_board)[:256]] == cells

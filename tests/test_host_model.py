@@ -80,7 +80,7 @@ def _candidates_from_tables(blob, h, level, neighbour_colours, order, w):
     """Decodes a level descriptor and returns (kind, candidate bits, placed sides):
     pair-table row for the first two placed neighbours & side masks of the others.
     A row is an occupancy word (bit w: word w is not zero) and kw 32-bit words."""
-    d = blob[h["desc"] + 8 * level: h["desc"] + 8 * level + 8]
+    d = blob[h["desc"] + 16 * level: h["desc"] + 16 * level + 16]
     kind, kw, nextra = (d[0] >> 8) & 3, d[0] & 0xFF, (d[0] >> 13) & 7
     pos = order[level]
 
