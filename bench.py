@@ -521,6 +521,8 @@ def main():
     ap.add_argument("--full", action="store_true", help="run all slices (the complete count) and print per-seed totals")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
+    ap.add_argument("--stack-placement", type=int, default=0,
+                    help="DFS stack: 0 library default, 1 shared 32-bit, 2 shared 16-bit, 3 global memory")
     ap.add_argument("--host-loop", action="store_true",
                     help="launch each DFS round from the host, one puzzle after another (the default runs each "
                          "puzzle's rounds as one CUDA graph, puzzles on concurrent streams)")
@@ -575,7 +577,8 @@ def main():
     # plan runs as one CUDA graph (every DFS round launched by the device) on a stream
     # of its own, so the rounds of one puzzle fill the GPU while another drains.
     graphs = not args.host_loop
-    plans = [native.BtPlan([p], split_depth=DEPTH, device=local_rank, use_graph=int(graphs)) for p in puzzles]
+    plans = [native.BtPlan([p], split_depth=DEPTH, device=local_rank, use_graph=int(graphs),
+                           stack_placement=args.stack_placement) for p in puzzles]
     counts = [pl.subtrees() for pl in plans]
     total_subtrees = sum(counts)
     flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.int32, device="cuda")

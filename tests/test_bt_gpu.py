@@ -369,3 +369,18 @@ def test_resume_solutions_results_bin_equals_reference_build():
         found, sols, res = native.bt_resume_solutions(npz, trans, capacity=4096)
         assert found == rec["solutions"] and res.nodes == rec["nodes"], rec["name"]
         assert hashlib.sha256(_results_bin(pz, order, sols, res.nodes)).hexdigest() == rec["results_sha256"], rec["name"]
+
+
+@pytest.mark.parametrize("placement", [1, 2, 3])
+def test_stack_placements_equal_reference_build(placement):
+    """Every placement of the DFS stack (shared 32-bit, shared 16-bit, global) gives the
+    reference build's counts, with work handed between threads (small split budget)."""
+    recs = [r for r in REF_RECORDS if r["group"] in ("config0", "random", "quirk")]
+    for rec in recs:
+        pz = Puzzle.from_csv(rec["csv"])
+        npz = native.NativePuzzle(pz.width, pz.height, pz.colors, order=_ref_order(rec, pz))
+        for tp in (1, 2):  # tables in global, then shared memory
+            r = native.bt_count(npz, split_depth=min(4, pz.nb_pieces - 1), split_budget=64,
+                                stack_placement=placement, table_placement=tp)
+            assert r.status == native.EMP_OK
+            assert (r.nodes, r.solutions) == (rec["nodes"], rec["solutions"]), (rec["name"], tp)
