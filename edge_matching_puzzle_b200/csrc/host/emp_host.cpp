@@ -228,6 +228,26 @@ void feature_CUDA_backtracker::run()
 {
     const auto start = std::chrono::steady_clock::now();
     emp_puzzle_owner puzzle(m_pieces, &m_strategy);
+    if (m_options.trace) {
+        // debug mode: the reference's own variable-space search, with the lines its
+        // kernel printed for every selection (src/CUDA_backtracker.cu:109-120)
+        std::vector<emp_vs_event> events(1u << 20);
+        uint64_t n_events = 0;
+        std::vector<uint32_t> board(m_pieces.size());
+        uint32_t found = 0;
+        m_out << "Launch kernels" << std::endl;
+        const emp_status st = emp_bt_variable_space(puzzle.get(), m_options.device, 0, m_options.timeout_ms,
+                                                    events.data(), events.size(), &n_events, board.data(), &found);
+        if (st < 0) throw_abi("emp_bt_variable_space", st, __LINE__);
+        for (uint64_t i = 0; i < std::min<uint64_t>(n_events, events.size()); ++i)
+            m_out << "Thread " << events[i].lane << " : selected variable " << events[i].variable << " at step "
+                  << events[i].step << std::endl;
+        if (found) m_out << situation_string(m_pieces.width, m_pieces.height, board.data()) << std::endl;
+        else m_out << "No solution" << std::endl;
+        const std::chrono::duration<double> elapsed = std::chrono::steady_clock::now() - start;
+        m_out << "Total elapsed time: " << elapsed.count() << "s" << std::endl;
+        return;
+    }
     emp_bt_config cfg{};
     cfg.device = m_options.device;
     cfg.split_depth = m_options.split_depth;

@@ -116,6 +116,7 @@ class feature_if {
 // Settings the reference hard-codes; the defaults reproduce its behaviour.
 struct feature_options {
     std::string initial_situation;  // new_strategy, CUDA_backtracker: resume from this situation string
+    bool trace = false;             // CUDA_backtracker: the reference's variable-space search and its trace
     bool stop_at_first = false;     // backtracker: stop at the first solution found
     uint32_t split_depth = 0;       // backtracker: 0 = library default
     uint64_t push_budget = 0;       // glutton: stop after this many placements (0 = none)

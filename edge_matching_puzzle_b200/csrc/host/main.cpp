@@ -13,6 +13,9 @@
 //                             situation string s (emp_strategy::set_initial_state)
 //   --enable_gui=...          accepted and ignored (there is no GUI here)
 //   --hint                    accepted and ignored
+//   --trace=true              CUDA_backtracker: run the reference's variable-space search
+//                             instead and print its "Thread L : selected variable V at
+//                             step S" lines (a debug mode, puzzles of at most 64 pieces)
 // Settings the reference hard-codes, exposed here:
 //   --stop_at_first=true|false  --split_depth=N  --push_budget=N  --timeout_ms=N  --device=N
 // Errors print "ERROR : <what> at <file>:<line>" and exit with -1.
@@ -63,7 +66,8 @@ int main(int argc, char** argv)
             throw emp_logic_error("usage: edge_matching_puzzle <definition> <ressources> <feature_name> [--name=value]",
                                   __LINE__, __FILE__);
         static const char* known[] = {"strategy", "enable_gui", "dump_file", "initial_situation", "hint",
-                                      "stop_at_first", "split_depth", "push_budget", "timeout_ms", "device"};
+                                      "stop_at_first", "split_depth", "push_budget", "timeout_ms", "device",
+                                      "trace"};
         for (const auto& kv : named) {
             bool ok = false;
             for (const char* k : known) ok = ok || kv.first == k;
@@ -79,6 +83,7 @@ int main(int argc, char** argv)
             options.timeout_ms = static_cast<uint32_t>(parse_u64("timeout_ms", named["timeout_ms"]));
         if (named.count("device")) options.device = static_cast<int>(parse_u64("device", named["device"]));
         if (named.count("initial_situation")) options.initial_situation = named["initial_situation"];
+        if (named.count("trace")) options.trace = parse_bool(named["trace"]);
 
         const emp_piece_set pieces = parse_pieces(positional[0]);
         std::cout << pieces.size() << " pieces loaded" << std::endl;

@@ -89,6 +89,10 @@ class BtSolution(ctypes.Structure):
     _fields_ = [("node_index", ctypes.c_uint64), ("board", ctypes.c_uint32 * 256)]
 
 
+class VsEvent(ctypes.Structure):
+    _fields_ = [("lane", ctypes.c_uint32), ("variable", ctypes.c_uint32), ("step", ctypes.c_uint32)]
+
+
 class TuneResult(ctypes.Structure):
     _fields_ = [
         ("best", BtConfig),
@@ -148,6 +152,9 @@ SIGNATURES = {
     "emp_puzzle_export_tables": (ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint32), ctypes.c_uint64,
                                                   u64p]),
     "emp_bt_count": (ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(BtConfig), ctypes.POINTER(BtResult)]),
+    "emp_bt_variable_space": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_uint64, ctypes.c_uint32,
+                                               ctypes.POINTER(VsEvent), ctypes.c_uint64, u64p,
+                                               ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint32)]),
     "emp_bt_resume": (ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint16), ctypes.c_uint32,
                                        ctypes.POINTER(BtConfig), ctypes.POINTER(BtResult)]),
     "emp_bt_resume_solutions": (ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint16), ctypes.c_uint32,
@@ -273,6 +280,19 @@ def bt_count(puzzle: NativePuzzle, **kw) -> BtResult:
     cfg = bt_config(**kw)
     check(load().emp_bt_count(puzzle.handle, ctypes.byref(cfg), ctypes.byref(r)))
     return r
+
+
+def bt_variable_space(puzzle: NativePuzzle, capacity: int = 4096, max_selections: int = 0, timeout_ms: int = 0,
+                      device: int = -1):
+    """emp_bt_variable_space (debug mode): ([(lane, variable, step)], board or None, status)."""
+    ev = (VsEvent * max(capacity, 1))()
+    ne = ctypes.c_uint64()
+    board = (ctypes.c_uint32 * puzzle.n)()
+    found = ctypes.c_uint32()
+    st = check(load().emp_bt_variable_space(puzzle.handle, device, max_selections, timeout_ms, ev, capacity,
+                                            ctypes.byref(ne), board, ctypes.byref(found)))
+    events = [(ev[i].lane, ev[i].variable, ev[i].step) for i in range(min(ne.value, capacity))]
+    return events, (list(board) if found.value else None), st
 
 
 def bt_resume(puzzle: NativePuzzle, situation: Sequence[int], **kw) -> BtResult:

@@ -207,6 +207,25 @@ emp_status emp_bt_resume_solutions(emp_puzzle puzzle, const uint16_t *situation,
                                    const emp_bt_config *config, emp_bt_solution *out, uint64_t capacity,
                                    uint64_t *found, emp_bt_result *result);
 
+/* Debug mode: the reference's own CUDA_backtracker search, the variable-space
+ * single-warp backtracker of src/CUDA_backtracker.cu:67-178 (variables and
+ * transition vectors of include/emp_variable_generator.h:335-621 and
+ * include/system_equation_for_CUDA.h:70-173), row-major puzzles of at most 64
+ * pieces.  Each selection is an event, the kernel's "Thread L : selected variable
+ * V at step S" line; *found = 1 and board[position] = (piece id-1)<<2 |
+ * orientation when it reached a solution (the reference's first solution, which
+ * the exhaustive search's first_solution also gives).  max_selections > 0 and
+ * timeout_ms (0 = 60 s) bound the run (EMP_INCOMPLETE). */
+typedef struct emp_vs_event {
+    uint32_t lane;               /* the elected lane */
+    uint32_t variable;           /* step << 10 | lane << 5 | bit */
+    uint32_t step;
+} emp_vs_event;
+
+emp_status emp_bt_variable_space(emp_puzzle puzzle, int device, uint64_t max_selections, uint32_t timeout_ms,
+                                 emp_vs_event *events, uint64_t capacity, uint64_t *n_events, uint32_t *board,
+                                 uint32_t *found);
+
 /* Split form of the batch call: plan (upload + prefix expansion), run (kernel
  * launch on a stream, asynchronous), results (synchronise + download). */
 typedef struct emp_bt_plan_t *emp_bt_plan;

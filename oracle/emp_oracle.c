@@ -1183,3 +1183,158 @@ int op_gm_run(op_puzzle *p, uint64_t budget, uint64_t push_budget, op_gm_result 
     free(g);
     return 0;
 }
+
+/* ------------------------------------------------------------------ */
+/* Variable-space backtracker of the reference's CUDA_backtracker feature, as a
+ * sequential restatement of its single-warp kernel (src/CUDA_backtracker.cu:67-178)
+ * with the variables of emp_variable_generator::create_variables
+ * (include/emp_variable_generator.h:335-525, no hints, empty situation) and the
+ * transition vectors of system_equation_for_CUDA::prepare_transitions /
+ * prepare_initial (include/system_equation_for_CUDA.h:70-173).
+ *
+ * A capability is 32 words: word 8*o + x/32, bit x%32 for (x, orientation o), where x
+ * is a piece index for the first n capabilities (one per position, in row-major
+ * order) and a position for the next n (one per piece).  Level l of the stack holds
+ * 2n capabilities; levels above 0 start zeroed and keep whatever an earlier attempt
+ * wrote, as the kernel's stack does (a piece already used at this level keeps a
+ * stale capability, which the piece check reads). */
+#define VS_W 32u
+
+typedef struct { uint32_t pos, piece, o; } vs_var;
+
+static void vs_clear(uint32_t *cap, uint32_t x, uint32_t o) { cap[8 * o + x / 32] &= ~(1u << (x % 32)); }
+static void vs_set(uint32_t *cap, uint32_t x, uint32_t o) { cap[8 * o + x / 32] |= 1u << (x % 32); }
+
+int op_vs_trace(op_puzzle *p, uint32_t max_events, uint32_t *ev_lane, uint32_t *ev_var, uint32_t *ev_step,
+                uint32_t *n_events, uint32_t *solution_board, uint64_t max_selections)
+{
+    build_table(p);
+    const uint32_t n = p->n, w = p->w, h = p->h, cs = p->cs, B = p->border_id;
+    if (n > 256) return -1;
+    /* variables per position, in the kind bitfield's ffs order */
+    vs_var *vars = (vs_var *)calloc((size_t)n * 1024, sizeof(vs_var));
+    uint32_t nv = 0;
+    uint32_t *pos_first = (uint32_t *)calloc(n + 1, sizeof(uint32_t));
+    for (uint32_t pos = 0; pos < n; ++pos) {
+        const uint32_t x = pos % w, y = pos / w;
+        pos_first[pos] = nv;
+        const uint32_t E = x == w - 1 ? B : 0, N = y == 0 ? B : 0, W = x == 0 ? B : 0, S = y == h - 1 ? B : 0;
+        const uint32_t code = (((((E << cs) | N) << cs) | W) << cs) | S;
+        if (code > p->max_code || p->table_off[code] == UINT32_MAX) continue;
+        const uint64_t *tab = p->table_pool + p->table_off[code];
+        const uint32_t k = p->table_kind[code];
+        for (uint32_t t = 0; t < p->kind_bits[k]; ++t) {
+            if (!bf_get(tab, t)) continue;
+            const uint32_t bin = p->binary[k][t] >> (4 * cs);
+            vars[nv].pos = pos;
+            vars[nv].piece = bin >> 2;
+            vars[nv].o = bin & 3u;
+            ++nv;
+        }
+    }
+    pos_first[n] = nv;
+    /* transition vectors, indexed by variable number */
+    const size_t capw = (size_t)2 * n * VS_W;
+    uint32_t *trans = (uint32_t *)malloc(sizeof(uint32_t) * capw * (nv ? nv : 1));
+    memset(trans, 0xFF, sizeof(uint32_t) * capw * (nv ? nv : 1));
+    int32_t *var_of = (int32_t *)malloc(sizeof(int32_t) * (size_t)n * 1024);
+    for (size_t i = 0; i < (size_t)n * 1024; ++i) var_of[i] = -1;
+    for (uint32_t v = 0; v < nv; ++v) var_of[vars[v].pos * 1024 + vars[v].o * 256 + vars[v].piece] = (int32_t)v;
+    for (uint32_t v = 0; v < nv; ++v) {
+        uint32_t *T = trans + capw * v;
+        for (uint32_t u = pos_first[vars[v].pos]; u < pos_first[vars[v].pos + 1]; ++u) {
+            vs_clear(T + VS_W * vars[v].pos, vars[u].piece, vars[u].o);
+            vs_clear(T + VS_W * (n + vars[u].piece), vars[v].pos, vars[u].o);
+        }
+        for (uint32_t u = 0; u < nv; ++u) {
+            if (vars[u].piece != vars[v].piece) continue;
+            vs_clear(T + VS_W * (n + vars[v].piece), vars[u].pos, vars[u].o);
+            vs_clear(T + VS_W * vars[u].pos, vars[v].piece, vars[u].o);
+        }
+    }
+    /* incompatible neighbours (emp_variable_generator.h:558-621) */
+    for (uint32_t y = 0; y < h; ++y)
+        for (uint32_t x = 0; x < w; ++x)
+            for (int dir = 0; dir < 2; ++dir) {
+                if (dir == 0 && x + 1 >= w) continue;
+                if (dir == 1 && y + 1 >= h) continue;
+                const uint32_t p1 = y * w + x, p2 = dir == 0 ? p1 + 1 : p1 + w;
+                const uint32_t side1 = dir == 0 ? 1u : 2u, side2 = dir == 0 ? 3u : 0u;
+                for (uint32_t a = pos_first[p1]; a < pos_first[p1 + 1]; ++a)
+                    for (uint32_t b = pos_first[p2]; b < pos_first[p2 + 1]; ++b) {
+                        const vs_var *v1 = &vars[a], *v2 = &vars[b];
+                        if (v1->piece == v2->piece) continue;
+                        if (p->col[v1->piece][(side1 + v1->o) & 3] == p->col[v2->piece][(side2 + v2->o) & 3]) continue;
+                        uint32_t *T1 = trans + capw * a, *T2 = trans + capw * b;
+                        vs_clear(T1 + VS_W * p2, v2->piece, v2->o);
+                        vs_clear(T1 + VS_W * (n + v2->piece), p2, v2->o);
+                        vs_clear(T2 + VS_W * p1, v1->piece, v1->o);
+                        vs_clear(T2 + VS_W * (n + v1->piece), p1, v1->o);
+                    }
+            }
+    /* stack: n+1 levels of 2n capabilities, level 0 from prepare_initial */
+    uint32_t *lev = (uint32_t *)calloc(capw * (n + 1), sizeof(uint32_t));
+    for (uint32_t v = 0; v < nv; ++v) {
+        vs_set(lev + VS_W * vars[v].pos, vars[v].piece, vars[v].o);
+        vs_set(lev + VS_W * (n + vars[v].piece), vars[v].pos, vars[v].o);
+    }
+    uint32_t *stack_var = (uint32_t *)calloc(n, sizeof(uint32_t));
+    uint32_t ne = 0, step = 0;
+    uint64_t selections = 0;
+    int found = 0;
+    do {
+        uint32_t *avail = lev + capw * step + VS_W * step;
+        uint32_t lane = VS_W;
+        for (uint32_t l = 0; l < VS_W; ++l)
+            if (avail[l]) { lane = l; break; }
+        if (lane == VS_W) { --step; continue; } /* step 0 wraps and ends the loop */
+        const uint32_t bit = (uint32_t)__builtin_ctz(avail[lane]);
+        const uint32_t var = (step << 10) | (lane << 5) | bit;
+        const uint32_t piece = (lane % 8) * 32 + bit;
+        if (ne < max_events) { ev_lane[ne] = lane; ev_var[ne] = var; ev_step[ne] = step; }
+        ++ne;
+        stack_var[step] = var;
+        avail[lane] &= ~(1u << bit);
+        if (step == n - 1) { found = 1; break; }
+        if (max_selections && ++selections >= max_selections) break;
+        const int32_t vi = var_of[var];
+        const uint32_t *S = lev + capw * step, *T = trans + capw * (vi >= 0 ? vi : 0);
+        uint32_t *R = lev + capw * (step + 1);
+        int valid = vi >= 0;
+        for (uint32_t q = step + 1; q < n && valid; ++q) {
+            uint32_t any = 0, r[VS_W];
+            for (uint32_t l = 0; l < VS_W; ++l) { r[l] = S[VS_W * q + l] & T[VS_W * q + l]; any |= r[l]; }
+            if (any) memcpy(R + VS_W * q, r, sizeof(r));
+            else valid = 0;
+        }
+        /* pieces below, then above, the selected one (src/CUDA_backtracker.cu:28-58,
+         * called at :155-164 with the transition vector in the place of the situation
+         * as well, so a piece's capability becomes the transition's own) */
+        for (int pass = 0; pass < 2 && valid; ++pass) {
+            const uint32_t q0 = pass ? piece + 1 : 0, q1 = pass ? n : piece;
+            for (uint32_t q = q0; q < q1 && valid; ++q) {
+                const uint32_t *Sq = T + VS_W * (n + q);
+                uint32_t any_s = 0;
+                for (uint32_t l = 0; l < VS_W; ++l) any_s |= Sq[l];
+                if (!any_s) continue;
+                uint32_t any = 0, r[VS_W];
+                for (uint32_t l = 0; l < VS_W; ++l) { r[l] = Sq[l] & T[VS_W * (n + q) + l]; any |= r[l]; }
+                if (any) memcpy(R + VS_W * (n + q), r, sizeof(r));
+                else valid = 0;
+            }
+        }
+        if (valid) {
+            memset(R + VS_W * (n + piece), 0, sizeof(uint32_t) * VS_W);
+            ++step;
+        }
+    } while (step < n);
+    *n_events = ne;
+    for (uint32_t i = 0; i < n; ++i) solution_board[i] = 0xFFFFFFFFu;
+    if (found)
+        for (uint32_t s = 0; s < n; ++s) {
+            const uint32_t var = stack_var[s], lane = (var >> 5) & 31u, bit = var & 31u;
+            solution_board[s] = (((lane % 8) * 32 + bit) << 2) | (lane / 8);
+        }
+    free(stack_var); free(lev); free(var_of); free(trans); free(pos_first); free(vars);
+    return found ? 0 : 1;
+}

@@ -134,6 +134,17 @@ typedef struct {
  * pushes, checked at the top of each level (0: none). */
 int op_gm_run(op_puzzle *p, uint64_t budget, uint64_t push_budget, op_gm_result *out);
 
+/* The reference's variable-space CUDA backtracker (feature CUDA_backtracker,
+ * src/CUDA_backtracker.cu:67-178 with include/system_equation_for_CUDA.h:70-173 and
+ * include/emp_variable_generator.h:335-621), row-major order, restated
+ * sequentially.  Every selection is an event (elected lane, variable id
+ * step<<10 | lane<<5 | bit, step): the kernel's "Thread L : selected variable V at
+ * step S" lines.  solution_board[position] = (piece id-1)<<2 | orientation of the
+ * first solution (0xFFFFFFFF when none).  max_selections > 0 stops after that many
+ * selections.  Returns 0 when a solution was found, 1 otherwise, -1 on bad input. */
+int op_vs_trace(op_puzzle *p, uint32_t max_events, uint32_t *ev_lane, uint32_t *ev_var, uint32_t *ev_step,
+                uint32_t *n_events, uint32_t *solution_board, uint64_t max_selections);
+
 #ifdef __cplusplus
 }
 #endif

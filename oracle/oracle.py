@@ -80,6 +80,8 @@ def lib():
                                 ctypes.c_char_p, ctypes.c_size_t]
         L.op_bt_resume.argtypes = [vp, ctypes.POINTER(u32), ctypes.POINTER(ctypes.c_uint16), u32, u64,
                                    ctypes.POINTER(BtResult), ctypes.c_char_p]
+        L.op_vs_trace.argtypes = [vp, u32, ctypes.POINTER(u32), ctypes.POINTER(u32), ctypes.POINTER(u32),
+                                  ctypes.POINTER(u32), ctypes.POINTER(u32), u64]
         L.op_bt_expand.restype = u64
         L.op_bt_expand.argtypes = [vp, ctypes.POINTER(u32), u32, ctypes.POINTER(ctypes.c_uint16), u64,
                                    ctypes.POINTER(u64), ctypes.POINTER(u64)]
@@ -166,6 +168,18 @@ class OraclePuzzle:
         if st:
             raise ValueError(f"situation not reachable (status {st})")
         return r
+
+    def vs_trace(self, max_events: int = 4096, max_selections: int = 0):
+        """The reference's variable-space CUDA backtracker restated: (events, board) with
+        events (lane, variable id, step) and the first solution's board (None if none)."""
+        la, va, st = ((ctypes.c_uint32 * max_events)() for _ in range(3))
+        ne = ctypes.c_uint32()
+        board = (ctypes.c_uint32 * self.n)()
+        r = lib().op_vs_trace(self._p, max_events, la, va, st, ctypes.byref(ne), board, max_selections)
+        if r < 0:
+            raise ValueError("puzzle too large")
+        ev = [(la[i], va[i], st[i]) for i in range(min(ne.value, max_events))]
+        return ev, (list(board) if r == 0 else None)
 
     def expand(self, depth: int, order=None, max_prefixes: int = 0):
         nn, ss = ctypes.c_uint64(), ctypes.c_uint64()

@@ -7,7 +7,8 @@ Reads, from the reference project (read-only):
   tests/new_strategy_*/test.info                    expected stdout lines (spiral order)
   tests/new_strategy_*/references/results.bin       solution dumps
   tests/CUDA_glutton_max_*/test.info                glutton max final boards
-  tests_CUDA/backtracker_*/test.info                row-major first solutions
+  tests_CUDA/backtracker_*/test.info                row-major first solutions and, for 3_3, the
+                                                    variable-space kernel's selection lines
   tests/dump_solutions_*/test.info                  FSM-engine totals (cross-check only)
 The JSON is committed; the tests never read the reference at run time.
 """
@@ -36,7 +37,7 @@ def main():
         sys.exit("usage: make_reference_golden.py /path/to/reference")
     ref = sys.argv[1]
     data = {"source": "reference project tests and doc/example", "puzzles": {}, "new_strategy": {},
-            "glutton_max": {}, "backtracker_first_solution": {}, "dump_solutions": {}}
+            "glutton_max": {}, "backtracker_first_solution": {}, "backtracker_trace": {}, "dump_solutions": {}}
     for name in ("3_3", "4_4", "5_5", "5_5_bis"):
         with open(os.path.join(ref, "doc", "example", name + ".txt")) as f:
             data["puzzles"][name] = f.read()
@@ -47,8 +48,9 @@ def main():
         data["new_strategy"][name] = {"strategy": "spiral", "expected_stdout": expected_lines(os.path.join(t, "test.info")),
                                       "results_bin_b64": base64.b64encode(rb).decode()}
         data["glutton_max"][name] = expected_lines(os.path.join(ref, "tests", "CUDA_glutton_max_" + name, "test.info"))
-        data["backtracker_first_solution"][name] = expected_lines(
-            os.path.join(ref, "tests_CUDA", "backtracker_" + name, "test.info"))[-1]
+        bt_lines = expected_lines(os.path.join(ref, "tests_CUDA", "backtracker_" + name, "test.info"))
+        data["backtracker_first_solution"][name] = bt_lines[-1]
+        data["backtracker_trace"][name] = bt_lines[:-1]
         data["dump_solutions"][name] = expected_lines(os.path.join(ref, "tests", "dump_solutions_" + name, "test.info"))
     with open(os.path.join(HERE, "reference_vectors.json"), "w") as f:
         json.dump(data, f, indent=1)

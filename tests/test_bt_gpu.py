@@ -384,3 +384,20 @@ def test_stack_placements_equal_reference_build(placement):
                                 stack_placement=placement, table_placement=tp)
             assert r.status == native.EMP_OK
             assert (r.nodes, r.solutions) == (rec["nodes"], rec["solutions"]), (rec["name"], tp)
+
+
+@pytest.mark.parametrize("name", ["3_3", "4_4", "5_5"])
+def test_variable_space_debug_mode(reference_vectors, name):
+    """emp_bt_variable_space: the reference's own CUDA_backtracker search on the GPU, its
+    selection lines for 3x3 (tests_CUDA/backtracker_3_3) and first solutions, and every
+    selection equal to the oracle's restatement."""
+    pz = Puzzle.from_csv(reference_vectors["puzzles"][name])
+    events, board, st = native.bt_variable_space(native.NativePuzzle(pz.width, pz.height, pz.colors),
+                                                 capacity=1 << 16)
+    assert st == native.EMP_OK and board is not None
+    assert board_string(pz.width, pz.height, board) == reference_vectors["backtracker_first_solution"][name]
+    want_events, want_board = OraclePuzzle(pz.width, pz.height, pz.colors).vs_trace(max_events=1 << 16)
+    assert events == want_events and board == want_board
+    if reference_vectors["backtracker_trace"][name]:
+        assert [f"Thread {l} : selected variable {v} at step {s}" for l, v, s in events] == \
+            reference_vectors["backtracker_trace"][name]

@@ -180,3 +180,18 @@ def test_new_strategy_initial_situation_matches_reference_build(cli, tmp_path):
         assert rc == 0, out
         assert f"Total situations explored : {rec['nodes']}" in out and f"Nb solutions : {rec['solutions']}" in out
         assert hashlib.sha256(dump.read_bytes()).hexdigest() == rec["results_sha256"], rec["name"]
+
+
+@pytest.mark.gpu
+def test_backtracker_trace_mode_lines(cli, example, reference_vectors):
+    """--trace=true: the lines of tests_CUDA/backtracker_3_3/test.info, in order."""
+    rc, out = run(cli, example("3_3"), "ressources", "CUDA_backtracker", "--enable_gui=false", "--trace=true")
+    assert rc == 0, out
+    expected = reference_vectors["backtracker_trace"]["3_3"] + [reference_vectors["backtracker_first_solution"]["3_3"]]
+    got = [l for l in out if l.startswith("Thread ") or l == expected[-1]]
+    assert got == expected, out
+
+
+def test_trace_mode_refuses_other_orders(cli, example):
+    rc, out = run(cli, example("3_3"), "ressources", "CUDA_backtracker", "--trace=true", "--strategy=spiral")
+    assert rc == 255 and "row-major" in out[-1], out

@@ -75,3 +75,17 @@ def test_split_counts_equal_whole_run(reference_vectors):
         count, nlo, slo, pref = op.expand(depth, max_prefixes=1 << 20)
         nhi, shi = op.subtrees_parallel(pref, depth, 0, count, 2)
         assert (nlo + nhi, slo + shi) == (whole.nodes, whole.solutions)
+
+
+@pytest.mark.parametrize("name", ["3_3", "4_4", "5_5"])
+def test_variable_space_search_golden(reference_vectors, name):
+    """The reference's variable-space CUDA_backtracker, restated (op_vs_trace): its
+    selection lines for 3x3 and its first solutions (tests_CUDA/backtracker_*)."""
+    pz = Puzzle.from_csv(reference_vectors["puzzles"][name])
+    events, board = OraclePuzzle(pz.width, pz.height, pz.colors).vs_trace(max_events=1 << 16)
+    assert board is not None
+    assert board_string(pz.width, pz.height, board) == reference_vectors["backtracker_first_solution"][name]
+    want = reference_vectors["backtracker_trace"][name]
+    if want:
+        got = [f"Thread {l} : selected variable {v} at step {s}" for l, v, s in events]
+        assert got == want
