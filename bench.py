@@ -14,9 +14,10 @@ Prints one JSON line (rank 0).  value: placements/s with the puzzle tables and t
 depth-12 prefixes resident on the device; e2e: the same metric through the one-shot
 public call emp_bt_count_batch with host-side inputs (table upload, prefix expansion,
 all rounds, result download inside the timed region).  The reference arm times the CPU
-restatement of emp_strategy (oracle/, the reference itself cannot be built here: its
-sibling libraries are not available) on all host cores over a bounded sample of the
-same subtrees.
+restatement of emp_strategy (oracle/emp_oracle.c, checked against the reference's own
+search built from its sources in oracle/_ref) on all host cores over a bounded sample
+of the same subtrees: the reference's search is single-threaded and has no way to
+search one subtree, so the multi-threaded restatement is the CPU path timed.
 """
 from __future__ import annotations
 
