@@ -300,7 +300,7 @@ emp_status resume_records(const emp_puzzle_t& pz, const uint16_t* situation, uin
         const uint32_t row = d[2] + ((ea >> ((d[1] >> 16) & 0xFFu)) & 31u) * (d[3] & 0xFFFFu) +
                              ((eb >> (d[1] >> 24)) & 31u) * (d[3] >> 16);
         std::vector<uint32_t> c(kw);
-        for (uint32_t w = 0; w < kw; ++w) c[w] = b[row + 1 + w] & av[aoff + w];
+        for (uint32_t w = 0; w < kw; ++w) c[w] = b[row + 2 + w] & av[aoff + w];
         for (uint32_t j = 0; j < nextra; ++j) {
             const uint32_t sd = (d[7] >> (2 * j)) & 3u, lev = (d[7] >> (8 + 8 * j)) & 0xFFu;
             const uint32_t* sm = &b[d[4] + (sd * ncol + facing(stk[lev], sd)) * kw];

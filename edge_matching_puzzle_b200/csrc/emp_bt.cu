@@ -100,7 +100,7 @@ __global__ void expand_kernel(BtLaunch P, const uint16_t* __restrict__ parents,
             const uint32_t kw = d.kw();
             const uint32_t row = d.row(stk[d.level_a()], stk[d.level_b()]);
             uint32_t R[kMaxKindWords];
-            for (uint32_t w = 0; w < kw; ++w) R[w] = ldg(tb + row + 1 + w) & av[d.aoff() + w];
+            for (uint32_t w = 0; w < kw; ++w) R[w] = ldg(tb + row + 2 + w) & av[d.aoff() + w];
             for (uint32_t j = 0; j < d.nextra(); ++j) {
                 const uint32_t sd = d.extra_side(j);
                 const uint32_t c = facing_colour(stk[d.extra_level(j)], sd);
@@ -257,6 +257,10 @@ struct Tab;
 template <>
 struct Tab<true> {
     static __device__ __forceinline__ uint32_t u32(const ThreadItem&, uint32_t off) { return g_smem[off]; }
+    static __device__ __forceinline__ uint32_t u16(const ThreadItem&, uint32_t off16)
+    {
+        return reinterpret_cast<const uint16_t*>(g_smem)[off16];
+    }
     static __device__ __forceinline__ LevelDesc desc(const ThreadItem& s, uint32_t L, bool ext)
     {
         const uint4* d = reinterpret_cast<const uint4*>(g_smem + s.desc_off + kDescWords * L);
@@ -269,6 +273,10 @@ struct Tab<true> {
 template <>
 struct Tab<false> {
     static __device__ __forceinline__ uint32_t u32(const ThreadItem& s, uint32_t off) { return ldg(s.tb + off); }
+    static __device__ __forceinline__ uint32_t u16(const ThreadItem& s, uint32_t off16)
+    {
+        return __ldg(reinterpret_cast<const uint16_t*>(s.tb) + off16);
+    }
     static __device__ __forceinline__ LevelDesc desc(const ThreadItem& s, uint32_t L, bool ext)
     {
         return load_desc(s.tb, s.desc_off, L, ext);
@@ -378,7 +386,7 @@ template <bool SM, int T, class S>
 __device__ __forceinline__ uint32_t candidate_word(const ThreadItem& s, const LevelDesc& d, uint32_t row, uint32_t w,
                                                    const S& stk, const uint32_t* av)
 {
-    uint32_t x = Tab<SM>::u32(s, row + 1 + w) & av[(d.aoff() + w) * T];
+    uint32_t x = Tab<SM>::u32(s, row + 2 + w) & av[(d.aoff() + w) * T];
     if (d.nextra()) {
         const uint32_t ncol = Tab<SM>::u32(s, H_NCOL), kw = d.kw();
         for (uint32_t j = 0; j < d.nextra(); ++j) {
@@ -390,17 +398,33 @@ __device__ __forceinline__ uint32_t candidate_word(const ThreadItem& s, const Le
     return x;
 }
 
-// First candidate t >= start of level L, and whether more may follow it.  The
-// unspilled walk visits only the row's occupied words; `more` is exact within
-// t's word and counts any later occupied row word.  Returns false when none.
+// Whether candidate t of level L passes the side masks of the level's third and
+// fourth placed neighbours (never present in row-major order).
+template <bool SM, class S>
+__device__ __forceinline__ bool extra_sides_allow(const ThreadItem& s, const LevelDesc& d, uint32_t t, const S& stk)
+{
+    const uint32_t ncol = Tab<SM>::u32(s, H_NCOL), kw = d.kw();
+    for (uint32_t j = 0; j < d.nextra(); ++j) {
+        const uint32_t sd = d.extra_side(j);
+        const uint32_t c = stk.template colour<SM>(s, d.extra_level(j), 5 * ((sd + 2) & 3u), j ? d.d11 : d.d10);
+        if (!((ldg(s.tb + d.d4 + (sd * ncol + c) * kw + (t >> 5)) >> (t & 31u)) & 1u)) return false;
+    }
+    return true;
+}
+
+// First candidate t >= start of level L, and whether more may follow it.
+// Unspilled levels walk their pair-table row's candidate list (the row's set bits
+// in ascending order) and test each candidate's piece in the availability words;
+// `more` says whether the list goes on after t.  A spilled level walks its exact
+// remaining set.  Returns false when there is no candidate.
 template <bool SM, int T, class S>
 __device__ __forceinline__ bool find_candidate(const BtLaunch& P, const ThreadItem& s, const LevelDesc& d, uint32_t L,
                                                uint32_t start, bool spilled, const S& stk, const uint32_t* av,
                                                const uint32_t* spill, uint32_t* t_out, bool* more_out)
 {
-    const uint32_t sw = start >> 5;
-    const uint32_t low = shl32(~0u, start & 31u);
     if (spilled) {
+        const uint32_t sw = start >> 5;
+        const uint32_t low = shl32(~0u, start & 31u);
         const uint32_t* sp = spill + L * P.max_kw;
         const uint32_t kw = d.kw();
         for (uint32_t w = sw; w < kw; ++w) {
@@ -417,17 +441,16 @@ __device__ __forceinline__ bool find_candidate(const BtLaunch& P, const ThreadIt
         return false;
     }
     const uint32_t row = level_row<SM>(s, d, stk);
-    uint32_t occ = Tab<SM>::u32(s, row) & shl32(~0u, sw);
-    while (occ) {
-        const uint32_t w = __ffs(occ) - 1;
-        occ &= occ - 1;
-        uint32_t x = candidate_word<SM, T>(s, d, row, w, stk, av);
-        if (w == sw) x &= low;
-        if (x) {
-            *t_out = 32 * w + __ffs(x) - 1;
-            *more_out = (x & (x - 1)) != 0 || occ != 0;
-            return true;
-        }
+    const uint32_t hdr = Tab<SM>::u32(s, row);
+    const uint32_t len = hdr >> 22, off = hdr & 0x3FFFFFu;
+    const uint32_t aoff = d.aoff();
+    for (uint32_t i = 0; i < len; ++i) {
+        const uint32_t t = Tab<SM>::u16(s, off + i);
+        if (t < start || !((av[(aoff + (t >> 5)) * T] >> (t & 31u)) & 1u)) continue;
+        if (d.nextra() && !extra_sides_allow<SM>(s, d, t, stk)) continue;
+        *t_out = t;
+        *more_out = i + 1 < len;
+        return true;
     }
     return false;
 }
@@ -446,19 +469,15 @@ __device__ __forceinline__ void pop_level(ThreadItem& s, const S& stk, uint32_t*
 }
 
 // One step of emp_strategy::specific_run (include/emp_strategy.h:352-401)
-// inside the thread's record: go up past the levels known to be exhausted, then
-// place the next candidate of the current level, or go up one level when it has
-// none.  Doing the known pops and the next try in the same step keeps the lanes
-// of a warp on the same (try) path.  Returns false once the record is exhausted.
+// inside the thread's record: place the next candidate of the current level, or go
+// up one level (without scanning when the level is known to be exhausted).  One pop
+// per step: a lane that went up several levels in one step would keep the others of
+// its warp idle.  Returns false once the record is exhausted.
 template <bool SM, int T, class S>
 __device__ __forceinline__ bool dfs_step(const BtLaunch& P, ThreadItem& s, S& stk, uint32_t* av, uint32_t* spill,
                                          bool* solved)
 {
-    while (s.pop) {
-        if (s.L == s.base) return false;
-        pop_level<SM, T>(s, stk, av);
-    }
-    {
+    if (!s.pop) {
         const LevelDesc d = Tab<SM>::desc(s, s.L, S::kNeedsKindTables);
         uint32_t t;
         bool more;
@@ -659,8 +678,12 @@ __global__ void __launch_bounds__(T) dfs_kernel(BtLaunch P)
     } else if (MODE == kStackShared32) {
         *reinterpret_cast<uint32_t**>(&stk.p) = g_smem + P.smem_tab_words + P.max_avail_words * T + tid;
     } else {
+        // warps 2j and 2j+1 share 32 words per level: lane l of the even warp takes the
+        // low half of word l, of the odd warp the high half, so the 32 lanes of a warp
+        // read 32 banks whatever levels they are at
         *reinterpret_cast<uint16_t**>(&stk.p) =
-            reinterpret_cast<uint16_t*>(g_smem + P.smem_tab_words + P.max_avail_words * T) + tid;
+            reinterpret_cast<uint16_t*>(g_smem + P.smem_tab_words + P.max_avail_words * T) +
+            ((tid & ~63u) | ((tid & 31u) << 1) | ((tid >> 5) & 1u));
     }
     uint32_t* spill = P.spill + (size_t)(blockIdx.x * T + tid) * P.max_levels * P.max_kw;
     ThreadItem s;

@@ -257,8 +257,11 @@ void build_device_tables(const PuzzleModel& m, const std::vector<LevelPlan>& pla
             }
         }
     }
-    // pair tables, one per distinct (kind, base, paired sides) class; a row is an
-    // occupancy word (bit w: candidate word w is not zero) and the kw candidate words
+    // pair tables, one per distinct (kind, base, paired sides) class.  A row is a
+    // list header (u16 offset of the row's candidate list | length << 22), an
+    // occupancy word (bit w: candidate word w is not zero) and the kw candidate
+    // words; the candidate lists (every set bit of the row in ascending order, u16)
+    // follow the last class, inside the hot prefix the kernels stage.
     align(b, 4);
     t.pair_off = static_cast<uint32_t>(b.size());
     struct Key {
@@ -271,6 +274,7 @@ void build_device_tables(const PuzzleModel& m, const std::vector<LevelPlan>& pla
     };
     std::vector<std::pair<Key, uint32_t>> classes;
     std::vector<uint32_t> level_pair(m.n);
+    std::vector<std::pair<uint32_t, std::vector<uint16_t>>> lists;  // (header word, candidates)
     for (uint32_t L = 0; L < m.n; ++L) {
         const LevelPlan& lp = plan[L];
         Key key{lp.kind, std::min<uint32_t>(lp.nplaced, 2), lp.nplaced > 0 ? lp.side[0] : 0u,
@@ -291,18 +295,32 @@ void build_device_tables(const PuzzleModel& m, const std::vector<LevelPlan>& pla
                 for (uint32_t cb = 0; cb < nb; ++cb) {
                     const size_t head = b.size();
                     b.push_back(0);
+                    b.push_back(0);
+                    std::vector<uint16_t> cand;
                     for (uint32_t w = 0; w < kw; ++w) {
                         uint32_t v = lp.base[w];
                         if (key.arity >= 1) v &= side[k][(static_cast<size_t>(key.sa) * t.ncol + ca) * kw + w];
                         if (key.arity >= 2) v &= side[k][(static_cast<size_t>(key.sb) * t.ncol + cb) * kw + w];
                         b.push_back(v);
-                        if (v) b[head] |= 1u << w;
+                        if (v) b[head + 1] |= 1u << w;
+                        for (uint32_t x = v; x; x &= x - 1) cand.push_back(static_cast<uint16_t>(32 * w + __builtin_ctz(x)));
                     }
+                    lists.emplace_back(static_cast<uint32_t>(head), std::move(cand));
                 }
             classes.push_back({key, off});
         }
         level_pair[L] = off;
     }
+    // candidate lists, u16 entries two per word
+    std::vector<uint16_t> packed;
+    const size_t list_base = b.size();
+    for (auto& l : lists) {
+        const size_t at = 2 * list_base + packed.size();  // at < 2^22 and length < 2^10 for n <= 256
+        b[l.first] = static_cast<uint32_t>(at) | (static_cast<uint32_t>(l.second.size()) << 22);
+        packed.insert(packed.end(), l.second.begin(), l.second.end());
+    }
+    if (packed.size() % 2) packed.push_back(0);
+    for (size_t i = 0; i < packed.size(); i += 2) b.push_back(packed[i] | (static_cast<uint32_t>(packed[i + 1]) << 16));
     // level descriptors
     align(b, 4);
     t.desc_off = static_cast<uint32_t>(b.size());
@@ -361,7 +379,7 @@ void build_device_tables(const PuzzleModel& m, const std::vector<LevelPlan>& pla
         // facing colour of the neighbour at side s sits at bits 5*((s+2)&3) of its stack word
         const uint32_t shift_a = arity > 0 ? 5 * ((lp.side[0] + 2u) & 3u) : 0u;
         const uint32_t shift_b = arity > 1 ? 5 * ((lp.side[1] + 2u) & 3u) : 0u;
-        const uint32_t row = t.kw[k] + 1;  // words per pair-table row
+        const uint32_t row = t.kw[k] + 2;  // words per pair-table row
         const uint32_t stride_b = arity > 1 ? row : 0u;
         const uint32_t stride_a = arity > 1 ? row * t.ncol : (arity > 0 ? row : 0u);
         d[0] = t.kw[k] | (k << 8) | (nextra << 13) | (t.aoff[k] << 16);

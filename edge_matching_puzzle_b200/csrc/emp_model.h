@@ -95,8 +95,10 @@ struct LevelPlan {
 //   d1 levelA | levelB<<8 | shiftA<<16 | shiftB<<24 (bit offset of the
 //      neighbour's facing colour in its stack word)
 //   d2 pair table (word offset): rows [cA][cB] (2 placed), [cA] (1), one row (0);
-//      a row is an occupancy word (bit w set when word w is not zero) and kw
-//      words = frame-side masks & allowed orientations & placed-side masks
+//      a row is a list header (u16 offset of its candidate list | length << 22),
+//      an occupancy word (bit w set when word w is not zero) and kw words =
+//      frame-side masks & allowed orientations & placed-side masks; the candidate
+//      lists (the row's set bits in ascending order, u16) follow the pair tables
 //   d3 strideA | strideB<<16 (words per colour step of A and B; 0 when absent)
 //   d4 side[kind], d5 tinfo[kind], d6 extra[kind],
 //   d7 extra placed sides: side3 | side4<<2 | level3<<8 | level4<<16

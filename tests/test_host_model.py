@@ -79,7 +79,8 @@ def _words(blob, off, count):
 def _candidates_from_tables(blob, h, level, neighbour_colours, order, w):
     """Decodes a level descriptor and returns (kind, candidate bits, placed sides):
     pair-table row for the first two placed neighbours & side masks of the others.
-    A row is an occupancy word (bit w: word w is not zero) and kw 32-bit words."""
+    A row is a candidate-list header, an occupancy word (bit w: word w is not zero) and
+    kw 32-bit words."""
     d = blob[h["desc"] + 16 * level: h["desc"] + 16 * level + 16]
     kind, kw, nextra = (d[0] >> 8) & 3, d[0] & 0xFF, (d[0] >> 13) & 7
     pos = order[level]
@@ -102,8 +103,12 @@ def _candidates_from_tables(blob, h, level, neighbour_colours, order, w):
         sides.append(sb)
         assert d[1] >> 24 == 5 * ((sb + 2) % 4)
         row += neighbour_colours[sb] * stride_b
-    words = _words(blob, row + 1, kw)
-    assert blob[row] == sum(1 << i for i, v in enumerate(words) if v)
+    words = _words(blob, row + 2, kw)
+    assert blob[row + 1] == sum(1 << i for i, v in enumerate(words) if v)
+    # the row's candidate list: its set bits in ascending order (u16 entries)
+    off, length = blob[row] & 0x3FFFFF, blob[row] >> 22
+    listed = [(blob[(off + i) >> 1] >> (16 * ((off + i) & 1))) & 0xFFFF for i in range(length)]
+    assert listed == [32 * i + b for i, v in enumerate(words) for b in range(32) if (v >> b) & 1]
     for j in range(nextra):
         sd = (d[7] >> (2 * j)) & 3
         sides.append(sd)
