@@ -423,6 +423,13 @@ def run_glutton(args, rank, world, local_rank):
     print(json.dumps(out), flush=True)
 
 
+TTFS_TRAIN_SEEDS = range(1000, 1064)
+TTFS_EVAL_SEEDS = range(100, 132)
+TTFS_TIMEOUT_MS = 10000
+TTFS_WORKLOAD = ("time to a first solution of 32 seeded 8x8 puzzles (4 border / 8 interior colours, seeds "
+                 "100..131), split depth 12, stop at the first solution any thread finds (10 s limit); plain order "
+                 "against subtrees queued best first by the network trained on the GPU on the solver's solution "
+                 "paths of seeds 1000..1063; the ordering's scoring and sort count in its time")
 LEARN_TRAIN_SEEDS = range(1000, 1256)
 LEARN_EVAL_SEEDS = range(100, 164)
 LEARN_TIMEOUT_MS = 30000
@@ -433,33 +440,33 @@ LEARN_WORKLOAD = ("time to a first solution of 64 seeded 8x8 puzzles (4 border /
                   "its time)")
 
 
-def run_learned(args, rank, world, local_rank):
-    """Learned value ordering: median time and placements to a first solution, plain vs learned."""
+def ttfs_measure(local_rank, train_seeds, eval_seeds, epochs, timeout_ms, rows_out=None):
+    """Time to a first solution (stop at the first solution any thread finds), plain
+    order against the learned order, on 8x8 puzzles.  The network is trained on the
+    GPU, by the project's kernels, on the solution paths the solver itself finds for
+    the training seeds.  Returns the summary and the training report."""
     import torch
     from edge_matching_puzzle_b200 import native
     from edge_matching_puzzle_b200.puzzle import generate
-    torch.cuda.set_device(local_rank)
-    if rank != 0:
-        return
     t_train0 = time.perf_counter()
     train_h, boards = [], []
-    for s in LEARN_TRAIN_SEEDS:
+    for s in train_seeds:
         pz = generate(WIDTH, HEIGHT, BORDER, INTERIOR, s)
         h = native.NativePuzzle(WIDTH, HEIGHT, pz.colors)
-        r = native.bt_count(h, split_depth=DEPTH, stop_at_any=1, timeout_ms=LEARN_TIMEOUT_MS, device=local_rank)
+        r = native.bt_count(h, split_depth=DEPTH, stop_at_any=1, timeout_ms=timeout_ms, device=local_rank)
         if r.has_first_solution:
             train_h.append(h)
             boards.append(list(r.first_solution))
     model = native.Mlp(seed=1, device=local_rank)
-    rep = model.train(train_h, boards, epochs=args.learn_epochs, batch=1024, learning_rate=1e-3, max_level=DEPTH)
+    rep = model.train(train_h, boards, epochs=epochs, batch=1024, learning_rate=1e-3, max_level=DEPTH)
     train_s = time.perf_counter() - t_train0
     rows = []
-    for s in LEARN_EVAL_SEEDS:
+    for s in eval_seeds:
         pz = generate(WIDTH, HEIGHT, BORDER, INTERIOR, s)
         h = native.NativePuzzle(WIDTH, HEIGHT, pz.colors)
         out = {"seed": s}
         for arm in ("plain", "learned"):
-            plan = native.BtPlan([h], split_depth=DEPTH, stop_at_any=1, timeout_ms=LEARN_TIMEOUT_MS, device=local_rank)
+            plan = native.BtPlan([h], split_depth=DEPTH, stop_at_any=1, timeout_ms=timeout_ms, device=local_rank)
             order_ms = 0.0
             if arm == "learned":
                 torch.cuda.synchronize()
@@ -475,30 +482,41 @@ def run_learned(args, rank, world, local_rank):
                         "complete": r.status == native.EMP_OK}
             plan.close()
         rows.append(out)
+    if rows_out:
+        with open(rows_out, "w") as f:
+            for r in rows:
+                f.write(json.dumps(r) + "\n")
     solved = [r for r in rows if r["plain"]["found"] and r["learned"]["found"]]
     med = lambda xs: statistics.median(xs) if xs else None  # noqa: E731
     plain_ms = med([r["plain"]["ms"] for r in solved])
     learned_ms = med([r["learned"]["ms"] for r in solved])
-    if args.counts_out:
-        with open(args.counts_out, "w") as f:
-            for r in rows:
-                f.write(json.dumps(r) + "\n")
+    pn, ln = med([r["plain"]["nodes"] for r in solved]), med([r["learned"]["nodes"] for r in solved])
+    summary = {"puzzles": len(rows), "with_solution": len(solved), "plain_median_ms": plain_ms,
+               "learned_median_ms": learned_ms,
+               "speedup_median_time": plain_ms / learned_ms if plain_ms and learned_ms else None,
+               "plain_median_nodes": pn, "learned_median_nodes": ln,
+               "speedup_median_nodes": pn / ln if pn and ln else None,
+               "median_order_ms": med([r["learned"]["order_ms"] for r in solved]),
+               "train": {"puzzles": rep.puzzles, "samples": rep.samples, "epochs": rep.epochs,
+                         "first_loss": rep.first_loss, "last_loss": rep.last_loss, "seconds_incl_traces": train_s}}
+    return summary
+
+
+def run_learned(args, rank, world, local_rank):
+    """Learned value ordering: median time and placements to a first solution, plain vs learned."""
+    import torch
+    torch.cuda.set_device(local_rank)
+    if rank != 0:
+        return
+    sm = ttfs_measure(local_rank, LEARN_TRAIN_SEEDS, LEARN_EVAL_SEEDS, args.learn_epochs, LEARN_TIMEOUT_MS,
+                      args.counts_out)
     out = {
-        "metric": METRIC, "value": learned_ms, "unit": "ms to a first solution (median)", "n_gpus": 1,
-        "steps": len(rows), "warmup": 0, "ms_per_step": learned_ms, "higher_is_better": False, "scaling": "weak",
-        "vs_baseline": None, "dtype": "u64 search, bf16 network", "data": "synthetic",
-        "config": {"workload": LEARN_WORKLOAD, "puzzles_with_solution": len(solved), "puzzles": len(rows),
-                   "train": {"puzzles": rep.puzzles, "samples": rep.samples, "positives": rep.positives,
-                             "epochs": rep.epochs, "first_loss": rep.first_loss, "last_loss": rep.last_loss,
-                             "seconds_incl_traces": train_s}},
-        "plain_median_ms": plain_ms,
-        "learned_median_ms": learned_ms,
-        "speedup_median_time": plain_ms / learned_ms if plain_ms and learned_ms else None,
-        "plain_median_nodes": med([r["plain"]["nodes"] for r in solved]),
-        "learned_median_nodes": med([r["learned"]["nodes"] for r in solved]),
-        "median_order_ms": med([r["learned"]["order_ms"] for r in solved]),
-        "gpu_launches": None,
-        "e2e": None,
+        "metric": METRIC, "value": sm["learned_median_ms"], "unit": "ms to a first solution (median)", "n_gpus": 1,
+        "steps": sm["puzzles"], "warmup": 0, "ms_per_step": sm["learned_median_ms"], "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u64 search, bf16 network", "data": "synthetic",
+        "config": {"workload": LEARN_WORKLOAD, "puzzles_with_solution": sm["with_solution"], "puzzles": sm["puzzles"],
+                   "train": sm["train"]},
+        "ttfs": sm, "gpu_launches": None, "e2e": None,
     }
     print(json.dumps(out), flush=True)
 
@@ -538,6 +556,7 @@ def main():
     ap.add_argument("--full", action="store_true", help="run all slices (the complete count) and print per-seed totals")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
+    ap.add_argument("--no-ttfs", action="store_true", help="skip the time-to-first-solution leg (plain vs learned)")
     ap.add_argument("--stack-placement", type=int, default=0,
                     help="DFS stack: 0 library default, 1 shared 32-bit, 2 shared 16-bit, 3 global memory")
     ap.add_argument("--host-loop", action="store_true",
@@ -713,6 +732,12 @@ def main():
         e_sec, (e_nodes,) = reduce_time_and_counts(dist, "cuda", e_sec, [float(e_nodes)])
         e2e = {"value": e_nodes / e_sec, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h}
 
+    # ---------------- time to a first solution, plain vs learned order ----------------
+    ttfs = None
+    if rank == 0 and world == 1 and not args.no_ttfs:
+        ttfs = ttfs_measure(local_rank, TTFS_TRAIN_SEEDS, TTFS_EVAL_SEEDS, args.learn_epochs, TTFS_TIMEOUT_MS)
+        ttfs["workload"] = TTFS_WORKLOAD
+
     # ---------------- CPU baseline (oracle) and algorithmic work ----------------
     peaks, peak_kind = measured_peaks()
     cpu = None
@@ -763,6 +788,7 @@ def main():
             "clocks": clocks,
             "e2e": e2e,
             "cpu_baseline": cpu,
+            "ttfs": ttfs,
             "dfs": {"rounds_per_step": rounds / args.steps, "launch": "host loop" if not graphs else
                     "one CUDA graph per puzzle slice (device-side round loop), 16 concurrent streams",
                     "busy_frac": busy / ms if ms and not graphs else None},
