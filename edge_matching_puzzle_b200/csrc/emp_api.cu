@@ -289,8 +289,11 @@ emp_status resume_records(const emp_puzzle_t& pz, const uint16_t* situation, uin
     const uint32_t n = b[1], ncol = b[2], desc_off = b[14], init = b[21], aw = b[9];
     if (placed < 2 || placed >= n)
         return fail(EMP_ERR_INVALID, "emp_bt_resume: the situation must place between 2 and n-1 pieces");
-    std::vector<uint32_t> av(b.begin() + init, b.begin() + init + aw), stk(n, 0);
-    std::vector<std::vector<uint32_t>> rem(placed);
+    auto u64at = [&](size_t off) { return static_cast<uint64_t>(b[off]) | (static_cast<uint64_t>(b[off + 1]) << 32); };
+    std::vector<uint64_t> av(aw);
+    for (uint32_t w = 0; w < aw; ++w) av[w] = u64at(init + 2 * w);
+    std::vector<uint32_t> stk(n, 0);
+    std::vector<std::vector<uint64_t>> rem(placed);
     std::vector<uint8_t> spilled(placed, 0);
     auto facing = [&](uint32_t e, uint32_t side) { return (e >> (5 * ((side + 2) & 3u))) & 31u; };
     for (uint32_t l = 0; l < placed; ++l) {
@@ -299,51 +302,54 @@ emp_status resume_records(const emp_puzzle_t& pz, const uint16_t* situation, uin
         const uint32_t ea = stk[d[1] & 0xFFu], eb = stk[(d[1] >> 8) & 0xFFu];
         const uint32_t row = d[2] + ((ea >> ((d[1] >> 16) & 0xFFu)) & 31u) * (d[3] & 0xFFFFu) +
                              ((eb >> (d[1] >> 24)) & 31u) * (d[3] >> 16);
-        std::vector<uint32_t> c(kw);
-        for (uint32_t w = 0; w < kw; ++w) c[w] = b[row + 2 + w] & av[aoff + w];
+        std::vector<uint64_t> c(kw);
+        for (uint32_t w = 0; w < kw; ++w) c[w] = u64at(row + 2 * w) & av[aoff + w];
         for (uint32_t j = 0; j < nextra; ++j) {
             const uint32_t sd = (d[7] >> (2 * j)) & 3u, lev = (d[7] >> (8 + 8 * j)) & 0xFFu;
-            const uint32_t* sm = &b[d[4] + (sd * ncol + facing(stk[lev], sd)) * kw];
-            for (uint32_t w = 0; w < kw; ++w) c[w] &= sm[w];
+            const size_t sm = d[4] + static_cast<size_t>((sd * ncol + facing(stk[lev], sd)) * kw) * 2;
+            for (uint32_t w = 0; w < kw; ++w) c[w] &= u64at(sm + 2 * w);
         }
         const uint32_t want = situation[l];
         uint32_t t = ~0u;
         while (t != want) {
             t = ~0u;
             for (uint32_t w = 0; w < kw && t == ~0u; ++w)
-                if (c[w]) t = 32 * w + static_cast<uint32_t>(__builtin_ctz(c[w]));
+                if (c[w]) t = 64 * w + static_cast<uint32_t>(__builtin_ctzll(c[w]));
             if (t == ~0u)
                 return fail(EMP_ERR_INVALID, "emp_bt_resume: the situation's piece at level " + std::to_string(l) +
                                                  " is not reachable in the search order");
             const uint32_t ti = b[d[5] + t];
             if ((ti >> 20) & 1u) {  // select_piece with an identical mask (emp_position_strategy.h:197-200)
-                for (uint32_t w = 0; w < kw; ++w) c[w] &= b[d[6] + t * kw + w];
+                for (uint32_t w = 0; w < kw; ++w) c[w] &= u64at(d[6] + static_cast<size_t>(t) * kw * 2 + 2 * w);
                 spilled[l] = 1;
             } else {
-                c[t >> 5] &= ~(1u << (t & 31u));
+                c[t >> 6] &= ~(uint64_t(1) << (t & 63u));
             }
         }
         rem[l] = c;
-        av[aoff + (t >> 5)] &= ~(0xFu << (t & 28u));
+        av[aoff + (t >> 6)] &= ~(uint64_t(0xF) << (t & 60u));
         stk[l] = b[d[5] + t] & 0xFFFFFu;
     }
     recs.clear();
     count = 0;
-    auto emit = [&](uint32_t len, uint32_t start, const std::vector<uint32_t>* rest) {
+    auto emit = [&](uint32_t len, uint32_t start, const std::vector<uint64_t>* rest) {
         std::vector<uint32_t> r(rec_words, 0);
         r[0] = static_cast<uint32_t>(count);
         r[2] = len | (start << 16);
         r[3] = rest ? (1u << 16) : 0u;
         for (uint32_t j = 0; j < len; ++j) r[4 + (j >> 1)] |= static_cast<uint32_t>(situation[j]) << (16 * (j & 1));
         if (rest)
-            for (uint32_t w = 0; w < rest->size() && w < max_kw; ++w) r[rec_words - max_kw + w] = (*rest)[w];
+            for (uint32_t w = 0; w < rest->size() && w < max_kw; ++w) {
+                r[rec_words - 2 * max_kw + 2 * w] = static_cast<uint32_t>((*rest)[w]);
+                r[rec_words - 2 * max_kw + 2 * w + 1] = static_cast<uint32_t>((*rest)[w] >> 32);
+            }
         recs.insert(recs.end(), r.begin(), r.end());
         ++count;
     };
     emit(placed - 1, 0, nullptr);
     for (uint32_t l = placed - 1; l-- > 1;) {
         bool any = false;
-        for (uint32_t v : rem[l]) any = any || v;
+        for (uint64_t v : rem[l]) any = any || v;
         if (any) emit(l, situation[l] + 1u, spilled[l] ? &rem[l] : nullptr);
     }
     return EMP_OK;
@@ -426,17 +432,17 @@ emp_status create_plan(const emp_puzzle* puzzles, uint32_t count, const emp_bt_c
     // launch geometry: the block size with the most resident warps per SM
     cudaDeviceProp prop;
     CUDA_TRY(cudaGetDeviceProperties(&prop, pl->device));
-    if (pl->max_kw > 32) return fail(EMP_ERR_UNSUPPORTED, "puzzle kinds wider than 32 candidate words");
+    if (pl->max_kw > 16) return fail(EMP_ERR_UNSUPPORTED, "puzzle kinds wider than 16 64-bit words");
     if (pl->cfg.stack_placement > 3)
         return fail(EMP_ERR_INVALID, "stack_placement must be 0 (default), 1, 2 or 3");
     pl->stack_mode = pl->cfg.stack_placement ? static_cast<int>(pl->cfg.stack_placement) : emp::kStackShared16;
     std::vector<uint32_t> candidates;
     if (pl->cfg.threads_per_block) candidates.push_back(pl->cfg.threads_per_block);
-    else candidates = {64, 128, 256, 512};
+    else candidates = {128, 256, 512};
     int best_warps = 0;
     for (uint32_t threads : candidates) {
         const void* fn = emp::dfs_kernel_symbol(pl->max_kw, pl->smem_tab_words != 0, threads, pl->stack_mode);
-        if (!fn) return fail(EMP_ERR_INVALID, "threads_per_block must be 64, 128, 256 or 512");
+        if (!fn) return fail(EMP_ERR_INVALID, "threads_per_block must be 128, 256 or 512");
         const size_t smem =
             emp::dfs_smem_bytes(pl->max_levels, pl->max_avail, threads, pl->smem_tab_words, pl->stack_mode);
         if (smem > static_cast<size_t>(prop.sharedMemPerBlockOptin)) continue;
@@ -453,7 +459,7 @@ emp_status create_plan(const emp_puzzle* puzzles, uint32_t count, const emp_bt_c
     }
     if (!best_warps)
         return fail(EMP_ERR_UNSUPPORTED, "per-thread DFS state does not fit shared memory; use fewer threads per block");
-    CUDA_TRY(pl->spill.alloc(sizeof(uint32_t) * static_cast<size_t>(pl->blocks) * pl->threads * pl->max_levels *
+    CUDA_TRY(pl->spill.alloc(sizeof(uint64_t) * static_cast<size_t>(pl->blocks) * pl->threads * pl->max_levels *
                              pl->max_kw));
     if (pl->stack_mode == emp::kStackGlobal32)
         CUDA_TRY(pl->stack.alloc(sizeof(uint32_t) * static_cast<size_t>(pl->blocks) * pl->threads * pl->max_levels));

@@ -11,13 +11,11 @@
 //      subtree ids from a global queue (one atomic per warp, distributed with
 //      ballot/shuffle) and walks it with its stack in shared memory.
 //
-// Per-thread DFS state lives in shared memory, thread-interleaved so that a
-// warp touching "its" entries hits 32 distinct banks:
-//   stk[L*T + tid]  = more << 31 | t << 21 | spilled << 20 | colours of the placed piece
-//   av[w*T + tid]   = 32-bit availability words of all three kinds
-// Candidate sets are 32-bit words (8 pieces x 4 orientations each).  A level's
-// pair-table row starts with an occupancy word (bit w: candidate word w is not
-// zero), so a try reads only the words that can hold a candidate.
+// Per-thread DFS state is thread-interleaved so that a warp touching "its" entries
+// hits 32 distinct banks: 64-bit availability words of the three kinds in shared
+// memory and a stack with one entry per level (placements below).  A level's
+// candidate words are computed in full, unrolled over a compile-time word count:
+// data-dependent loops over words cost more in idle lanes than they save.
 // The identical-piece case needs the exact remaining-candidate set of a level
 // once a transition with a non-trivial mask has been tried there; such a level
 // keeps its set in a per-thread global scratch row (spill) until it is left.
@@ -37,22 +35,14 @@ namespace {
 
 constexpr unsigned kFull = 0xFFFFFFFFu;
 constexpr uint32_t kMaxExpandDepth = 64;
-constexpr uint32_t kMaxAvailWords = 40;   // 32-bit availability words, three kinds (256 pieces)
-constexpr uint32_t kMaxKindWords = 32;    // 32-bit words of one kind (256 pieces x 4 orientations)
+constexpr uint32_t kMaxAvailWords = 24;   // 64-bit availability words, three kinds
+constexpr uint32_t kMaxKindWords = 16;    // 64-bit words of one kind (256 pieces)
 
 __device__ __forceinline__ uint64_t global_ns()
 {
     uint64_t t;
     asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
     return t;
-}
-
-// 32-bit shift left whose amount saturates at 32 (PTX clamps shift amounts)
-__device__ __forceinline__ uint32_t shl32(uint32_t v, uint32_t n)
-{
-    uint32_t r;
-    asm("shl.b32 %0, %1, %2;" : "=r"(r) : "r"(v), "r"(n));
-    return r;
 }
 
 // ---------------------------------------------------------------------------
@@ -83,15 +73,15 @@ __global__ void expand_kernel(BtLaunch P, const uint16_t* __restrict__ parents,
         }
         const uint32_t* tb = P.tables + P.puzzle_offset[pz];
         const uint32_t n = ldg(tb + H_N), ncol = ldg(tb + H_NCOL), desc_off = ldg(tb + H_DESC);
-        uint32_t av[kMaxAvailWords];
+        uint64_t av[kMaxAvailWords];
         uint32_t stk[kMaxExpandDepth];
         const uint32_t aw = ldg(tb + H_AWORDS), init = ldg(tb + H_INIT);
-        for (uint32_t w = 0; w < aw; ++w) av[w] = ldg(tb + init + w);
+        for (uint32_t w = 0; w < aw; ++w) av[w] = ldg64(tb + init + 2 * w);
         const uint16_t* pre = parents + i * level;
         for (uint32_t l = 0; l < level; ++l) {
             const LevelDesc d = load_desc(tb, desc_off, l);
             const uint32_t t = pre[l];
-            av[d.aoff() + (t >> 5)] &= ~(0xFu << (t & 28u));
+            av[d.aoff() + (t >> 6)] &= ~(0xFull << (t & 60u));
             stk[l] = ldg(tb + d.d5 + t) & 0xFFFFFu;
         }
         uint32_t cnt = 0;
@@ -99,18 +89,18 @@ __global__ void expand_kernel(BtLaunch P, const uint16_t* __restrict__ parents,
             const LevelDesc d = load_desc(tb, desc_off, level);
             const uint32_t kw = d.kw();
             const uint32_t row = d.row(stk[d.level_a()], stk[d.level_b()]);
-            uint32_t R[kMaxKindWords];
-            for (uint32_t w = 0; w < kw; ++w) R[w] = ldg(tb + row + 2 + w) & av[d.aoff() + w];
+            uint64_t R[kMaxKindWords];
+            for (uint32_t w = 0; w < kw; ++w) R[w] = ldg64(tb + row + 2 * w) & av[d.aoff() + w];
             for (uint32_t j = 0; j < d.nextra(); ++j) {
                 const uint32_t sd = d.extra_side(j);
                 const uint32_t c = facing_colour(stk[d.extra_level(j)], sd);
-                const uint32_t* sm = tb + d.d4 + (sd * ncol + c) * kw;
-                for (uint32_t w = 0; w < kw; ++w) R[w] &= ldg(sm + w);
+                const uint32_t* sm = tb + d.d4 + ((sd * ncol + c) * kw) * 2;
+                for (uint32_t w = 0; w < kw; ++w) R[w] &= ldg64(sm + 2 * w);
             }
             uint64_t out = mode ? offsets[i] : 0;
             for (uint32_t w = 0; w < kw; ++w) {
                 while (R[w]) {
-                    const uint32_t t = w * 32 + __ffs(R[w]) - 1;
+                    const uint32_t t = w * 64 + __ffsll(R[w]) - 1;
                     if (mode) {
                         uint16_t* c = children + out * (level + 1);
                         for (uint32_t l = 0; l < level; ++l) c[l] = pre[l];
@@ -124,10 +114,10 @@ __global__ void expand_kernel(BtLaunch P, const uint16_t* __restrict__ parents,
                         break;
                     }
                     if ((ldg(tb + d.d5 + t) >> 20) & 1u) {
-                        const uint32_t* ex = tb + d.d6 + t * kw;
-                        for (uint32_t ww = 0; ww < kw; ++ww) R[ww] &= ldg(ex + ww);
+                        const uint32_t* ex = tb + d.d6 + t * kw * 2;
+                        for (uint32_t ww = 0; ww < kw; ++ww) R[ww] &= ldg64(ex + 2 * ww);
                     } else {
-                        R[w] &= ~(1u << (t & 31));
+                        R[w] &= ~(1ull << (t & 63));
                     }
                 }
             }
@@ -220,12 +210,12 @@ __global__ void scan_apply(const uint32_t* __restrict__ in, uint64_t n, const ui
 //
 // record words: [0,1] subtree id (for per-subtree counts), [2] len | start<<16,
 // [3] puzzle | spilled<<16 | empty<<17, [4..] transitions (u16 pairs), then
-// the remaining set of level len (max_kw 32-bit words).
+// the remaining set of level len (max_kw 64-bit words as u32 pairs).
 //
 // Per-thread state, thread-interleaved with a compile-time block size T (a warp
 // touching its own entries hits distinct banks and every address is base +
 // immediate):
-//   av[w*T + tid]  = 32-bit availability words of the three kinds (shared memory)
+//   av[w*T + tid]  = 64-bit availability words of the three kinds (shared memory)
 //   the DFS stack, one entry per level, in one of three placements (StackMode):
 //     kStackShared32: shared memory, more<<31 | t<<21 | spilled<<20 | colours of
 //                     the placed piece (5 bits per side)
@@ -234,8 +224,7 @@ __global__ void scan_apply(const uint32_t* __restrict__ in, uint64_t n, const ui
 //                     the transition table of its kind instead
 //     kStackGlobal32: the 32-bit form in global memory (cached in L1), which leaves
 //                     shared memory to the tables and the availability words
-//   more: candidates may remain after t (exact within t's word, over-approximated
-//   by the row's occupancy beyond it).
+//   more: candidates remained after t when it was placed.
 struct ThreadItem {
     uint64_t orig;
     const uint32_t* tb;
@@ -257,9 +246,9 @@ struct Tab;
 template <>
 struct Tab<true> {
     static __device__ __forceinline__ uint32_t u32(const ThreadItem&, uint32_t off) { return g_smem[off]; }
-    static __device__ __forceinline__ uint32_t u16(const ThreadItem&, uint32_t off16)
+    static __device__ __forceinline__ uint64_t u64(const ThreadItem&, uint32_t off)
     {
-        return reinterpret_cast<const uint16_t*>(g_smem)[off16];
+        return reinterpret_cast<const unsigned long long*>(g_smem)[off >> 1];
     }
     static __device__ __forceinline__ LevelDesc desc(const ThreadItem& s, uint32_t L, bool ext)
     {
@@ -273,10 +262,7 @@ struct Tab<true> {
 template <>
 struct Tab<false> {
     static __device__ __forceinline__ uint32_t u32(const ThreadItem& s, uint32_t off) { return ldg(s.tb + off); }
-    static __device__ __forceinline__ uint32_t u16(const ThreadItem& s, uint32_t off16)
-    {
-        return __ldg(reinterpret_cast<const uint16_t*>(s.tb) + off16);
-    }
+    static __device__ __forceinline__ uint64_t u64(const ThreadItem& s, uint32_t off) { return ldg64(s.tb + off); }
     static __device__ __forceinline__ LevelDesc desc(const ThreadItem& s, uint32_t L, bool ext)
     {
         return load_desc(s.tb, s.desc_off, L, ext);
@@ -329,6 +315,14 @@ struct Stk<kStackShared16, T> {
     static constexpr bool kNeedsKindTables = true;
 };
 
+// 64-bit shift left whose amount saturates at 64 (PTX clamps shift amounts)
+__device__ __forceinline__ uint64_t shl_sat(uint64_t v, uint32_t n)
+{
+    uint64_t r;
+    asm("shl.b64 %0, %1, %2;" : "=l"(r) : "l"(v), "r"(n));
+    return r;
+}
+
 __device__ __forceinline__ uint32_t rec_t(const uint32_t* rec, uint32_t l)
 {
     return (rec[4 + (l >> 1)] >> (16 * (l & 1))) & 0xFFFFu;
@@ -336,7 +330,7 @@ __device__ __forceinline__ uint32_t rec_t(const uint32_t* rec, uint32_t l)
 
 template <bool SM, int T, class S>
 __device__ __forceinline__ void load_record(const BtLaunch& P, ThreadItem& s, const uint32_t* rec, S& stk,
-                                            uint32_t* av, uint32_t* spill)
+                                            uint64_t* av, uint64_t* spill)
 {
     using TB = Tab<SM>;
     s.orig = static_cast<uint64_t>(rec[0]) | (static_cast<uint64_t>(rec[1]) << 32);
@@ -348,17 +342,18 @@ __device__ __forceinline__ void load_record(const BtLaunch& P, ThreadItem& s, co
     s.n = TB::u32(s, H_N);
     s.desc_off = TB::u32(s, H_DESC);
     const uint32_t aw = TB::u32(s, H_AWORDS), init = TB::u32(s, H_INIT);
-    for (uint32_t w = 0; w < aw; ++w) av[w * T] = ldg(s.tb + init + w);
+    for (uint32_t w = 0; w < aw; ++w) av[w * T] = ldg64(s.tb + init + 2 * w);
     for (uint32_t l = 0; l < len; ++l) {
         const uint32_t d0 = TB::u32(s, s.desc_off + kDescWords * l);
         const uint32_t d5 = TB::u32(s, s.desc_off + kDescWords * l + 5);
         const uint32_t t = rec_t(rec, l);
-        av[((d0 >> 16) + (t >> 5)) * T] &= ~(0xFu << (t & 28u));
+        av[((d0 >> 16) + (t >> 6)) * T] &= ~(0xFull << (t & 60u));
         stk.put(l, t, false, 0u, S::kNeedsKindTables ? 0u : TB::u32(s, d5 + t));
     }
     if (s.spilled) {
         const uint32_t* R = rec + P.rec_r_off;
-        for (uint32_t w = 0; w < P.max_kw; ++w) spill[len * P.max_kw + w] = R[w];
+        for (uint32_t w = 0; w < P.max_kw; ++w)
+            spill[len * P.max_kw + w] = static_cast<uint64_t>(R[2 * w]) | (static_cast<uint64_t>(R[2 * w + 1]) << 32);
     }
     s.L = len;
     s.base = len;
@@ -369,102 +364,77 @@ __device__ __forceinline__ void load_record(const BtLaunch& P, ThreadItem& s, co
     s.active = true;
 }
 
-// Pair-table row of level L: its first two placed neighbours' facing colours
-// index it (a neighbour that is absent has stride 0).
-template <bool SM, class S>
-__device__ __forceinline__ uint32_t level_row(const ThreadItem& s, const LevelDesc& d, const S& stk)
+// Candidate words of level L (not yet masked by the resume bit): the level's
+// pair-table row (frame sides & the first two placed neighbours) & availability
+// & the side masks of further placed neighbours, or the spilled remaining set.
+template <int KW, bool SM, int T, class S>
+__device__ __forceinline__ void level_candidates(const BtLaunch& P, const ThreadItem& s, const LevelDesc& d,
+                                                 uint32_t L, bool spilled, const S& stk, const uint64_t* av,
+                                                 const uint64_t* spill, uint64_t* x)
 {
+    const uint32_t kw = d.kw();
+    if (spilled) {
+        const uint64_t* sp = spill + L * P.max_kw;
+#pragma unroll
+        for (int w = 0; w < KW; ++w) x[w] = (uint32_t)w < kw ? sp[w] : 0ull;
+        return;
+    }
     const uint32_t ca = stk.template colour<SM>(s, d.level_a(), d.shift_a(), d.d8);
     const uint32_t cb = stk.template colour<SM>(s, d.level_b(), d.shift_b(), d.d9);
-    return d.d2 + ca * d.stride_a() + cb * d.stride_b();
-}
-
-// Candidate word w of level L from its pair-table row (frame sides & the first
-// two placed neighbours), the availability, and the side masks of further placed
-// neighbours (never present in row-major order).
-template <bool SM, int T, class S>
-__device__ __forceinline__ uint32_t candidate_word(const ThreadItem& s, const LevelDesc& d, uint32_t row, uint32_t w,
-                                                   const S& stk, const uint32_t* av)
-{
-    uint32_t x = Tab<SM>::u32(s, row + 2 + w) & av[(d.aoff() + w) * T];
+    const uint32_t row = d.d2 + ca * d.stride_a() + cb * d.stride_b();
+    const uint64_t* a = av + d.aoff() * T;
+#pragma unroll
+    for (int w = 0; w < KW; ++w) x[w] = (uint32_t)w < kw ? Tab<SM>::u64(s, row + 2 * w) & a[w * T] : 0ull;
     if (d.nextra()) {
-        const uint32_t ncol = Tab<SM>::u32(s, H_NCOL), kw = d.kw();
+        const uint32_t ncol = Tab<SM>::u32(s, H_NCOL);
         for (uint32_t j = 0; j < d.nextra(); ++j) {
             const uint32_t sd = d.extra_side(j);
             const uint32_t c = stk.template colour<SM>(s, d.extra_level(j), 5 * ((sd + 2) & 3u), j ? d.d11 : d.d10);
-            x &= ldg(s.tb + d.d4 + (sd * ncol + c) * kw + w);
+            const uint32_t* sm = s.tb + d.d4 + ((sd * ncol + c) * kw) * 2;
+#pragma unroll
+            for (int w = 0; w < KW; ++w)
+                if ((uint32_t)w < kw) x[w] &= ldg64(sm + 2 * w);
         }
     }
-    return x;
 }
 
-// Whether candidate t of level L passes the side masks of the level's third and
-// fourth placed neighbours (never present in row-major order).
-template <bool SM, class S>
-__device__ __forceinline__ bool extra_sides_allow(const ThreadItem& s, const LevelDesc& d, uint32_t t, const S& stk)
+// Masks the words below bit `start`, finds the first candidate t and whether
+// more candidates follow it.  Returns false when there is none.
+template <int KW>
+__device__ __forceinline__ bool first_candidate(uint64_t* x, uint32_t start, uint32_t* t, bool* more)
 {
-    const uint32_t ncol = Tab<SM>::u32(s, H_NCOL), kw = d.kw();
-    for (uint32_t j = 0; j < d.nextra(); ++j) {
-        const uint32_t sd = d.extra_side(j);
-        const uint32_t c = stk.template colour<SM>(s, d.extra_level(j), 5 * ((sd + 2) & 3u), j ? d.d11 : d.d10);
-        if (!((ldg(s.tb + d.d4 + (sd * ncol + c) * kw + (t >> 5)) >> (t & 31u)) & 1u)) return false;
-    }
-    return true;
-}
-
-// First candidate t >= start of level L, and whether more may follow it.
-// Unspilled levels walk their pair-table row's candidate list (the row's set bits
-// in ascending order) and test each candidate's piece in the availability words;
-// `more` says whether the list goes on after t.  A spilled level walks its exact
-// remaining set.  Returns false when there is no candidate.
-template <bool SM, int T, class S>
-__device__ __forceinline__ bool find_candidate(const BtLaunch& P, const ThreadItem& s, const LevelDesc& d, uint32_t L,
-                                               uint32_t start, bool spilled, const S& stk, const uint32_t* av,
-                                               const uint32_t* spill, uint32_t* t_out, bool* more_out)
-{
-    if (spilled) {
-        const uint32_t sw = start >> 5;
-        const uint32_t low = shl32(~0u, start & 31u);
-        const uint32_t* sp = spill + L * P.max_kw;
-        const uint32_t kw = d.kw();
-        for (uint32_t w = sw; w < kw; ++w) {
-            uint32_t x = sp[w];
-            if (w == sw) x &= low;
-            if (x) {
-                *t_out = 32 * w + __ffs(x) - 1;
-                bool more = (x & (x - 1)) != 0;
-                for (uint32_t v = w + 1; v < kw && !more; ++v) more = sp[v] != 0;
-                *more_out = more;
-                return true;
-            }
+    bool found = false;
+    uint32_t fw = 0;
+    uint64_t fx = 0;
+#pragma unroll
+    for (int w = 0; w < KW; ++w) {
+        const int sh = static_cast<int>(start) - 64 * w;
+        x[w] &= shl_sat(~0ull, static_cast<uint32_t>(sh > 0 ? sh : 0));
+        if (!found && x[w]) {
+            found = true;
+            fw = w;
+            fx = x[w];
         }
-        return false;
     }
-    const uint32_t row = level_row<SM>(s, d, stk);
-    const uint32_t hdr = Tab<SM>::u32(s, row);
-    const uint32_t len = hdr >> 22, off = hdr & 0x3FFFFFu;
-    const uint32_t aoff = d.aoff();
-    for (uint32_t i = 0; i < len; ++i) {
-        const uint32_t t = Tab<SM>::u16(s, off + i);
-        if (t < start || !((av[(aoff + (t >> 5)) * T] >> (t & 31u)) & 1u)) continue;
-        if (d.nextra() && !extra_sides_allow<SM>(s, d, t, stk)) continue;
-        *t_out = t;
-        *more_out = i + 1 < len;
-        return true;
-    }
-    return false;
+    uint64_t rest = fx & (fx - 1);  // first word without t
+#pragma unroll
+    for (int w = 0; w < KW; ++w)
+        if ((uint32_t)w > fw) rest |= x[w];
+    *more = rest != 0;
+    *t = fw * 64 + __ffsll(fx) - 1;
+    return found;
 }
 
 // Goes up one level: gives back the piece placed there and resumes after it.
 template <bool SM, int T, class S>
-__device__ __forceinline__ void pop_level(ThreadItem& s, const S& stk, uint32_t* av)
+__device__ __forceinline__ void pop_level(ThreadItem& s, const S& stk, uint64_t* av)
 {
     --s.L;
     const uint32_t t = stk.t(s.L);
     s.spilled = stk.spilled(s.L);
     s.pop = !stk.more(s.L);
     const uint32_t aoff = Tab<SM>::u32(s, s.desc_off + kDescWords * s.L) >> 16;
-    av[(aoff + (t >> 5)) * T] |= 0xFu << (t & 28u);
+    av[(aoff + (t >> 6)) * T] |= 0xFull << (t & 60u);
     s.start = t + 1;
 }
 
@@ -473,38 +443,39 @@ __device__ __forceinline__ void pop_level(ThreadItem& s, const S& stk, uint32_t*
 // up one level (without scanning when the level is known to be exhausted).  One pop
 // per step: a lane that went up several levels in one step would keep the others of
 // its warp idle.  Returns false once the record is exhausted.
-template <bool SM, int T, class S>
-__device__ __forceinline__ bool dfs_step(const BtLaunch& P, ThreadItem& s, S& stk, uint32_t* av, uint32_t* spill,
+template <int KW, bool SM, int T, class S>
+__device__ __forceinline__ bool dfs_step(const BtLaunch& P, ThreadItem& s, S& stk, uint64_t* av, uint64_t* spill,
                                          bool* solved)
 {
     if (!s.pop) {
         const LevelDesc d = Tab<SM>::desc(s, s.L, S::kNeedsKindTables);
+        uint64_t x[KW];
+        level_candidates<KW, SM, T>(P, s, d, s.L, s.spilled != 0, stk, av, spill, x);
         uint32_t t;
         bool more;
-        if (find_candidate<SM, T>(P, s, d, s.L, s.start, s.spilled != 0, stk, av, spill, &t, &more)) {
+        if (first_candidate<KW>(x, s.start, &t, &more)) {
             const uint32_t ti = Tab<SM>::u32(s, d.d5 + t);
             if ((ti >> 20) & 1u) {
                 // select_piece with an identical mask that clears other candidates
                 // (emp_position_strategy.h:197-200): the level keeps its exact
                 // remaining set from now on
                 const uint32_t kw = d.kw();
-                uint32_t* sp = spill + s.L * P.max_kw;
-                const uint32_t* ex = s.tb + d.d6 + t * kw;
-                const uint32_t row = s.spilled ? 0u : level_row<SM>(s, d, stk);
-                const uint32_t tw = t >> 5;
-                bool rest = false;
-                for (uint32_t w = 0; w < kw; ++w) {
-                    uint32_t x = s.spilled ? sp[w] : candidate_word<SM, T>(s, d, row, w, stk, av);
-                    x &= ldg(ex + w);
-                    sp[w] = x;
-                    if (w > tw) rest |= x != 0;
-                    else if (w == tw) rest |= (x & shl32(~0u, (t & 31u) + 1)) != 0;
-                }
-                more = rest;
+                if (!s.spilled) level_candidates<KW, SM, T>(P, s, d, s.L, false, stk, av, spill, x);
+                const uint32_t* ex = s.tb + d.d6 + t * kw * 2;
+                uint64_t* sp = spill + s.L * P.max_kw;
+                uint64_t rest = 0;
+#pragma unroll
+                for (int w = 0; w < KW; ++w)
+                    if ((uint32_t)w < kw) {
+                        sp[w] = x[w] & ldg64(ex + 2 * w);
+                        const int sh = static_cast<int>(t + 1) - 64 * w;
+                        rest |= sp[w] & shl_sat(~0ull, static_cast<uint32_t>(sh > 0 ? sh : 0));
+                    }
+                more = rest != 0;
                 s.spilled = 1;
             }
-            uint32_t& aw = av[(d.aoff() + (t >> 5)) * T];
-            const uint32_t nib = 0xFu << (t & 28u);
+            uint64_t& aw = av[(d.aoff() + (t >> 6)) * T];
+            const uint64_t nib = 0xFull << (t & 60u);
             aw &= ~nib;
             stk.put(s.L, t, more, s.spilled, ti);
             ++s.nodes;
@@ -580,10 +551,10 @@ __device__ __forceinline__ void account(const BtLaunch& P, const ThreadItem& s)
 
 // Remaining candidates of level l (current level: from s.start unless it is
 // known exhausted; shallower levels: after their placed transition, when the
-// `more` bit says some may remain), with `av` holding level l's entry availability.
-template <bool SM, int T, class S>
+// `more` bit says some remain), with `av` holding level l's entry availability.
+template <int KW, bool SM, int T, class S>
 __device__ __forceinline__ bool level_has_work(const BtLaunch& P, const ThreadItem& s, uint32_t l, const S& stk,
-                                               const uint32_t* av, const uint32_t* spill, uint32_t* start_out,
+                                               const uint64_t* av, const uint64_t* spill, uint32_t* start_out,
                                                uint32_t* spilled_out)
 {
     uint32_t start, spilled;
@@ -601,19 +572,21 @@ __device__ __forceinline__ bool level_has_work(const BtLaunch& P, const ThreadIt
     *spilled_out = spilled;
     if (!maybe) return false;
     const LevelDesc d = Tab<SM>::desc(s, l, S::kNeedsKindTables);
+    uint64_t x[KW];
+    level_candidates<KW, SM, T>(P, s, d, l, spilled != 0, stk, av, spill, x);
     uint32_t t;
     bool more;
-    return find_candidate<SM, T>(P, s, d, l, start, spilled != 0, stk, av, spill, &t, &more);
+    return first_candidate<KW>(x, start, &t, &more);
 }
 
 template <bool SM, int T, class S>
-__device__ __forceinline__ void toggle_piece(const ThreadItem& s, uint32_t l, const S& stk, uint32_t* av,
+__device__ __forceinline__ void toggle_piece(const ThreadItem& s, uint32_t l, const S& stk, uint64_t* av,
                                              bool give_back)
 {
     const uint32_t aoff = Tab<SM>::u32(s, s.desc_off + kDescWords * l) >> 16;
     const uint32_t t = stk.t(l);
-    if (give_back) av[(aoff + (t >> 5)) * T] |= 0xFu << (t & 28u);
-    else av[(aoff + (t >> 5)) * T] &= ~(0xFu << (t & 28u));
+    if (give_back) av[(aoff + (t >> 6)) * T] |= 0xFull << (t & 60u);
+    else av[(aoff + (t >> 6)) * T] &= ~(0xFull << (t & 60u));
 }
 
 // Hands the remaining work of the thread's record to the next round: one
@@ -622,19 +595,19 @@ __device__ __forceinline__ void toggle_piece(const ThreadItem& s, uint32_t l, co
 // availability, and counts; pass 2 walks back down, writing records and taking
 // the pieces again, which leaves the state as it was.  Returns false when the
 // output queue is full (the thread then keeps the work).
-template <bool SM, int T, class S>
-__device__ bool split_record(const BtLaunch& P, ThreadItem& s, const S& stk, uint32_t* av, const uint32_t* spill)
+template <int KW, bool SM, int T, class S>
+__device__ bool split_record(const BtLaunch& P, ThreadItem& s, const S& stk, uint64_t* av, const uint64_t* spill)
 {
     uint32_t cnt = 0, start, spilled;
     for (uint32_t l = s.L + 1; l-- > s.base;) {
         if (l < s.L) toggle_piece<SM, T>(s, l, stk, av, true);
-        cnt += level_has_work<SM, T>(P, s, l, stk, av, spill, &start, &spilled);
+        cnt += level_has_work<KW, SM, T>(P, s, l, stk, av, spill, &start, &spilled);
     }
     const unsigned long long slot = cnt ? atomicAdd(P.out_tail, (unsigned long long)cnt) : 0ull;
     const bool fits = slot + cnt <= P.out_capacity;
     unsigned long long k = slot;
     for (uint32_t l = s.base; l <= s.L; ++l) {
-        if (level_has_work<SM, T>(P, s, l, stk, av, spill, &start, &spilled)) {
+        if (level_has_work<KW, SM, T>(P, s, l, stk, av, spill, &start, &spilled)) {
             if (fits) {
                 uint32_t* rec = P.out_rec + k * P.rec_words;
                 rec[0] = static_cast<uint32_t>(s.orig);
@@ -647,7 +620,11 @@ __device__ bool split_record(const BtLaunch& P, ThreadItem& s, const S& stk, uin
                     rec[4 + (j >> 1)] = lo | (hi << 16);
                 }
                 if (spilled)
-                    for (uint32_t w = 0; w < P.max_kw; ++w) rec[P.rec_r_off + w] = spill[l * P.max_kw + w];
+                    for (uint32_t w = 0; w < P.max_kw; ++w) {
+                        const uint64_t v = spill[l * P.max_kw + w];
+                        rec[P.rec_r_off + 2 * w] = static_cast<uint32_t>(v);
+                        rec[P.rec_r_off + 2 * w + 1] = static_cast<uint32_t>(v >> 32);
+                    }
             } else if (k < P.out_capacity) {
                 P.out_rec[k * P.rec_words + 3] = 1u << 17;  // reserved slot that fits: mark empty
             }
@@ -658,7 +635,7 @@ __device__ bool split_record(const BtLaunch& P, ThreadItem& s, const S& stk, uin
     return fits;
 }
 
-template <bool SM, int T, int MODE, int kStepsPerFetch>
+template <int KW, bool SM, int T, int MODE, int kStepsPerFetch>
 __global__ void __launch_bounds__(T) dfs_kernel(BtLaunch P)
 {
     const uint32_t tid = threadIdx.x, lane = tid & 31;
@@ -671,21 +648,21 @@ __global__ void __launch_bounds__(T) dfs_kernel(BtLaunch P)
     }
     // this thread's columns of the interleaved state: availability words, then
     // (shared placements) the stack
-    uint32_t* av = g_smem + P.smem_tab_words + tid;
+    uint64_t* av = reinterpret_cast<uint64_t*>(g_smem + P.smem_tab_words) + tid;
     Stk<MODE, T> stk;
     if (MODE == kStackGlobal32) {
         *reinterpret_cast<uint32_t**>(&stk.p) = P.stack + (size_t)blockIdx.x * T * P.max_levels + tid;
     } else if (MODE == kStackShared32) {
-        *reinterpret_cast<uint32_t**>(&stk.p) = g_smem + P.smem_tab_words + P.max_avail_words * T + tid;
+        *reinterpret_cast<uint32_t**>(&stk.p) = g_smem + P.smem_tab_words + 2 * P.max_avail_words * T + tid;
     } else {
         // warps 2j and 2j+1 share 32 words per level: lane l of the even warp takes the
         // low half of word l, of the odd warp the high half, so the 32 lanes of a warp
         // read 32 banks whatever levels they are at
         *reinterpret_cast<uint16_t**>(&stk.p) =
-            reinterpret_cast<uint16_t*>(g_smem + P.smem_tab_words + P.max_avail_words * T) +
+            reinterpret_cast<uint16_t*>(g_smem + P.smem_tab_words + 2 * P.max_avail_words * T) +
             ((tid & ~63u) | ((tid & 31u) << 1) | ((tid >> 5) & 1u));
     }
-    uint32_t* spill = P.spill + (size_t)(blockIdx.x * T + tid) * P.max_levels * P.max_kw;
+    uint64_t* spill = P.spill + (size_t)(blockIdx.x * T + tid) * P.max_levels * P.max_kw;
     ThreadItem s;
     s.active = false;
     bool alive = true;
@@ -739,7 +716,7 @@ __global__ void __launch_bounds__(T) dfs_kernel(BtLaunch P)
         for (int step = 0; step < kStepsPerFetch; ++step) {
             if (s.active) {
                 bool solved = false;
-                if (dfs_step<SM, T>(P, s, stk, av, spill, &solved)) {
+                if (dfs_step<KW, SM, T>(P, s, stk, av, spill, &solved)) {
                     if (solved) {
                         record_solution(P, s, stk);
                         if (P.sols) {
@@ -771,7 +748,7 @@ __global__ void __launch_bounds__(T) dfs_kernel(BtLaunch P)
 
         // ---- once the queue is empty, hand work back for the next round ----
         if (drained && P.item_budget && s.steps >= P.item_budget) {
-            if (split_record<SM, T>(P, s, stk, av, spill)) {
+            if (split_record<KW, SM, T>(P, s, stk, av, spill)) {
                 account(P, s);
                 s.active = false;
                 alive = false;
@@ -930,32 +907,44 @@ __global__ void record_prefix(const uint32_t* __restrict__ rec, uint32_t rec_wor
     for (uint32_t l = threadIdx.x; l < 256; l += blockDim.x) out[l] = l < len ? static_cast<uint16_t>(rec_t(r, l)) : 0xFFFFu;
 }
 
-template <int T, int MODE>
+template <int KW, int T, int MODE>
 const void* dfs_symbol(bool sm)
 {
-    return sm ? reinterpret_cast<const void*>(&dfs_kernel<true, T, MODE, 32>)
-              : reinterpret_cast<const void*>(&dfs_kernel<false, T, MODE, 32>);
+    return sm ? reinterpret_cast<const void*>(&dfs_kernel<KW, true, T, MODE, 32>)
+              : reinterpret_cast<const void*>(&dfs_kernel<KW, false, T, MODE, 32>);
+}
+
+// Word counts with a kernel: a puzzle runs with the smallest one that holds its
+// widest kind (8x8: 3 words, 12x12: 7 -> 8, 16x16: 13 -> 16).
+template <int T, int MODE>
+const void* dfs_symbol_kw(uint32_t max_kw, bool sm)
+{
+    if (max_kw <= 1) return dfs_symbol<1, T, MODE>(sm);
+    if (max_kw <= 2) return dfs_symbol<2, T, MODE>(sm);
+    if (max_kw <= 3) return dfs_symbol<3, T, MODE>(sm);
+    if (max_kw <= 4) return dfs_symbol<4, T, MODE>(sm);
+    if (max_kw <= 8) return dfs_symbol<8, T, MODE>(sm);
+    if (max_kw <= 16) return dfs_symbol<16, T, MODE>(sm);
+    return nullptr;
 }
 
 template <int T>
-const void* dfs_symbol_mode(bool sm, int mode)
+const void* dfs_symbol_mode(uint32_t max_kw, bool sm, int mode)
 {
     switch (mode) {
-        case kStackShared32: return dfs_symbol<T, kStackShared32>(sm);
-        case kStackShared16: return dfs_symbol<T, kStackShared16>(sm);
-        case kStackGlobal32: return dfs_symbol<T, kStackGlobal32>(sm);
+        case kStackShared32: return dfs_symbol_kw<T, kStackShared32>(max_kw, sm);
+        case kStackShared16: return dfs_symbol_kw<T, kStackShared16>(max_kw, sm);
+        case kStackGlobal32: return dfs_symbol_kw<T, kStackGlobal32>(max_kw, sm);
         default: return nullptr;
     }
 }
 
 const void* dfs_symbol_for(uint32_t max_kw, bool sm, uint32_t threads, int mode)
 {
-    if (max_kw > kMaxKindWords) return nullptr;
     switch (threads) {
-        case 64: return dfs_symbol_mode<64>(sm, mode);
-        case 128: return dfs_symbol_mode<128>(sm, mode);
-        case 256: return dfs_symbol_mode<256>(sm, mode);
-        case 512: return dfs_symbol_mode<512>(sm, mode);
+        case 128: return dfs_symbol_mode<128>(max_kw, sm, mode);
+        case 256: return dfs_symbol_mode<256>(max_kw, sm, mode);
+        case 512: return dfs_symbol_mode<512>(max_kw, sm, mode);
         default: return nullptr;
     }
 }
@@ -1027,11 +1016,11 @@ size_t dfs_smem_bytes(uint32_t max_levels, uint32_t max_avail_words, uint32_t th
 {
     const size_t stack = stack_mode == kStackShared32 ? 4 : (stack_mode == kStackShared16 ? 2 : 0);
     return static_cast<size_t>(tab_words) * sizeof(uint32_t) +
-           static_cast<size_t>(max_avail_words) * sizeof(uint32_t) * threads +
+           static_cast<size_t>(max_avail_words) * sizeof(uint64_t) * threads +
            ((static_cast<size_t>(max_levels) * stack * threads + 3) & ~size_t(3));
 }
 
-uint32_t record_words(uint32_t max_levels, uint32_t max_kw) { return 4 + (max_levels + 1) / 2 + max_kw; }
+uint32_t record_words(uint32_t max_levels, uint32_t max_kw) { return 4 + (max_levels + 1) / 2 + 2 * max_kw; }
 
 const void* dfs_kernel_symbol(uint32_t max_kw, bool smem_tables, uint32_t threads, int stack_mode)
 {

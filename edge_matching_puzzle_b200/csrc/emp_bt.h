@@ -53,9 +53,9 @@ struct BtLaunch {
     const uint64_t* puzzle_offset = nullptr;  // word offset of each puzzle blob
     uint32_t depth = 0;                       // split depth (prefix expansion)
     uint32_t max_levels = 0;                  // max pieces over the puzzles of the launch
-    uint32_t max_avail_words = 0;             // max 32-bit availability words (three kinds)
-    uint32_t max_kw = 0;                      // max 32-bit candidate words of one kind
-    uint32_t* spill = nullptr;                // [threads][max_levels][max_kw] remaining sets
+    uint32_t max_avail_words = 0;             // max 64-bit availability words (three kinds)
+    uint32_t max_kw = 0;                      // max 64-bit candidate words of one kind
+    uint64_t* spill = nullptr;                // [threads][max_levels][max_kw] remaining sets
     uint32_t smem_tab_words = 0;              // > 0: single puzzle, hot tables staged in shared memory
     // work records of this round and of the next one
     const uint32_t* in_rec = nullptr;

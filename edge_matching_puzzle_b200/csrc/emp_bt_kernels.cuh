@@ -10,7 +10,7 @@
 // removes the bits of its identical mask (:189-202).
 //
 // Table blob layout: emp_model.h (DeviceTables).  Candidate bit t =
-// kind_index*4 + orientation lives in 32-bit word t>>5, bit t&31.
+// kind_index*4 + orientation lives in 64-bit word t>>6, bit t&63.
 #pragma once
 
 #include "emp_layout.h"
@@ -27,6 +27,10 @@ enum : uint32_t {
 };
 
 __device__ __forceinline__ uint32_t ldg(const uint32_t* p) { return __ldg(p); }
+__device__ __forceinline__ uint64_t ldg64(const uint32_t* p)
+{
+    return __ldg(reinterpret_cast<const unsigned long long*>(p));
+}
 
 struct LevelDesc {
     uint32_t d0, d1, d2, d3, d4, d5, d6, d7;
@@ -45,7 +49,6 @@ struct LevelDesc {
     __device__ __forceinline__ uint32_t extra_side(uint32_t j) const { return (d7 >> (2 * j)) & 3u; }
     __device__ __forceinline__ uint32_t extra_level(uint32_t j) const { return (d7 >> (8 + 8 * j)) & 0xFFu; }
     // pair-table row of this level given the stack words of neighbours A and B
-    // (its occupancy word; the candidate words follow)
     __device__ __forceinline__ uint32_t row(uint32_t ea, uint32_t eb) const
     {
         return d2 + ((ea >> shift_a()) & 31u) * stride_a() + ((eb >> shift_b()) & 31u) * stride_b();

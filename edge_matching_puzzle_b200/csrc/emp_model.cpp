@@ -220,6 +220,14 @@ bool build_plan(const PuzzleModel& m, const std::vector<uint32_t>& order,
 
 namespace {
 
+inline void set_bit64(uint64_t* w, uint32_t i) { w[i >> 6] |= uint64_t(1) << (i & 63); }
+
+void push64(std::vector<uint32_t>& b, uint64_t v)
+{
+    b.push_back(static_cast<uint32_t>(v));
+    b.push_back(static_cast<uint32_t>(v >> 32));
+}
+
 void align(std::vector<uint32_t>& b, size_t words)
 {
     while (b.size() % words) b.push_back(0);
@@ -233,7 +241,7 @@ void build_device_tables(const PuzzleModel& m, const std::vector<LevelPlan>& pla
     t.n = m.n;
     t.ncol = m.border_id + 1;
     for (uint32_t k = 0; k < 3; ++k) {
-        t.kw[k] = m.kind_words[k];  // 32-bit words: 8 pieces x 4 orientations each
+        t.kw[k] = (4 * m.nb_kind(k) + 63) / 64;
         t.aoff[k] = t.avail_words;
         t.avail_words += t.kw[k];
         t.max_kw = std::max(t.max_kw, t.kw[k]);
@@ -242,7 +250,7 @@ void build_device_tables(const PuzzleModel& m, const std::vector<LevelPlan>& pla
     b.assign(kHeaderWords, 0);
     // side masks per kind: bit (ki,o) when side s of piece ki@o shows colour c
     // (c = border_id for a frame side), for allowed orientations only
-    std::array<std::vector<uint32_t>, 3> side;
+    std::array<std::vector<uint64_t>, 3> side;
     for (uint32_t k = 0; k < 3; ++k) {
         side[k].assign(static_cast<size_t>(4) * t.ncol * t.kw[k], 0);
         for (uint32_t ki = 0; ki < m.nb_kind(k); ++ki) {
@@ -252,16 +260,12 @@ void build_device_tables(const PuzzleModel& m, const std::vector<LevelPlan>& pla
                 for (uint32_t s = 0; s < 4; ++s) {
                     uint32_t c = m.colour(p, s, o);
                     if (!c) c = m.border_id;
-                    set_bit(&side[k][(static_cast<size_t>(s) * t.ncol + c) * t.kw[k]], 4 * ki + o);
+                    set_bit64(&side[k][(static_cast<size_t>(s) * t.ncol + c) * t.kw[k]], 4 * ki + o);
                 }
             }
         }
     }
-    // pair tables, one per distinct (kind, base, paired sides) class.  A row is a
-    // list header (u16 offset of the row's candidate list | length << 22), an
-    // occupancy word (bit w: candidate word w is not zero) and the kw candidate
-    // words; the candidate lists (every set bit of the row in ascending order, u16)
-    // follow the last class, inside the hot prefix the kernels stage.
+    // pair tables, one per distinct (kind, base, paired sides) class
     align(b, 4);
     t.pair_off = static_cast<uint32_t>(b.size());
     struct Key {
@@ -274,7 +278,6 @@ void build_device_tables(const PuzzleModel& m, const std::vector<LevelPlan>& pla
     };
     std::vector<std::pair<Key, uint32_t>> classes;
     std::vector<uint32_t> level_pair(m.n);
-    std::vector<std::pair<uint32_t, std::vector<uint16_t>>> lists;  // (header word, candidates)
     for (uint32_t L = 0; L < m.n; ++L) {
         const LevelPlan& lp = plan[L];
         Key key{lp.kind, std::min<uint32_t>(lp.nplaced, 2), lp.nplaced > 0 ? lp.side[0] : 0u,
@@ -288,45 +291,32 @@ void build_device_tables(const PuzzleModel& m, const std::vector<LevelPlan>& pla
                 break;
             }
         if (!found) {
+            align(b, 4);
             off = static_cast<uint32_t>(b.size());
             const uint32_t k = key.kind, kw = t.kw[k];
+            std::vector<uint64_t> base64(kw, 0);
+            for (uint32_t i = 0; i < 4 * m.nb_kind(k); ++i)
+                if ((lp.base[i >> 5] >> (i & 31)) & 1u) set_bit64(base64.data(), i);
             const uint32_t na = key.arity >= 1 ? t.ncol : 1, nb = key.arity >= 2 ? t.ncol : 1;
             for (uint32_t ca = 0; ca < na; ++ca)
-                for (uint32_t cb = 0; cb < nb; ++cb) {
-                    const size_t head = b.size();
-                    b.push_back(0);
-                    b.push_back(0);
-                    std::vector<uint16_t> cand;
+                for (uint32_t cb = 0; cb < nb; ++cb)
                     for (uint32_t w = 0; w < kw; ++w) {
-                        uint32_t v = lp.base[w];
+                        uint64_t v = base64[w];
                         if (key.arity >= 1) v &= side[k][(static_cast<size_t>(key.sa) * t.ncol + ca) * kw + w];
                         if (key.arity >= 2) v &= side[k][(static_cast<size_t>(key.sb) * t.ncol + cb) * kw + w];
-                        b.push_back(v);
-                        if (v) b[head + 1] |= 1u << w;
-                        for (uint32_t x = v; x; x &= x - 1) cand.push_back(static_cast<uint16_t>(32 * w + __builtin_ctz(x)));
+                        push64(b, v);
                     }
-                    lists.emplace_back(static_cast<uint32_t>(head), std::move(cand));
-                }
             classes.push_back({key, off});
         }
         level_pair[L] = off;
     }
-    // candidate lists, u16 entries two per word
-    std::vector<uint16_t> packed;
-    const size_t list_base = b.size();
-    for (auto& l : lists) {
-        const size_t at = 2 * list_base + packed.size();  // at < 2^22 and length < 2^10 for n <= 256
-        b[l.first] = static_cast<uint32_t>(at) | (static_cast<uint32_t>(l.second.size()) << 22);
-        packed.insert(packed.end(), l.second.begin(), l.second.end());
-    }
-    if (packed.size() % 2) packed.push_back(0);
-    for (size_t i = 0; i < packed.size(); i += 2) b.push_back(packed[i] | (static_cast<uint32_t>(packed[i + 1]) << 16));
     // level descriptors
     align(b, 4);
     t.desc_off = static_cast<uint32_t>(b.size());
     b.resize(b.size() + kDescWords * static_cast<size_t>(m.n), 0);
     // transition info
     for (uint32_t k = 0; k < 3; ++k) {
+        align(b, 2);
         t.tinfo_off[k] = static_cast<uint32_t>(b.size());
         const uint32_t bits = 4 * m.nb_kind(k);
         for (uint32_t e = 0; e < bits; ++e) {
@@ -350,24 +340,36 @@ void build_device_tables(const PuzzleModel& m, const std::vector<LevelPlan>& pla
     for (uint32_t k = 0; k < 3; ++k) {
         align(b, 4);
         t.side_off[k] = static_cast<uint32_t>(b.size());
-        b.insert(b.end(), side[k].begin(), side[k].end());
+        for (uint64_t v : side[k]) push64(b, v);
     }
     for (uint32_t k = 0; k < 3; ++k) {
+        align(b, 2);
         t.extra_off[k] = static_cast<uint32_t>(b.size());
         const uint32_t bits = 4 * m.nb_kind(k);
         for (uint32_t e = 0; e < bits; ++e) {
             const uint32_t* im = &m.idmask[k][static_cast<size_t>(e) * m.kind_words[k]];
             for (uint32_t w = 0; w < t.kw[k]; ++w) {
-                // bits past the kind's candidates stay 1, like the reference's all-ones init
-                const uint32_t pad = 32 * w + 32 > bits ? ~0u << (bits - 32 * w) : 0u;
-                b.push_back(im[w] | pad);
+                uint64_t v = 0;
+                for (uint32_t i = 0; i < 64; ++i) {
+                    const uint32_t bit = 64 * w + i;
+                    // bits past the kind's candidates stay 1, like the reference's all-ones init
+                    const bool one = bit >= bits || ((im[bit >> 5] >> (bit & 31)) & 1u);
+                    if (one) v |= uint64_t(1) << i;
+                }
+                push64(b, v);
             }
         }
     }
+    align(b, 2);
     t.init_off = static_cast<uint32_t>(b.size());
     for (uint32_t k = 0; k < 3; ++k) {
         const uint32_t bits = 4 * m.nb_kind(k);
-        for (uint32_t w = 0; w < t.kw[k]; ++w) b.push_back(32 * w + 32 <= bits ? ~0u : ~(~0u << (bits - 32 * w)));
+        for (uint32_t w = 0; w < t.kw[k]; ++w) {
+            uint64_t v = 0;
+            for (uint32_t i = 0; i < 64; ++i)
+                if (w * 64 + i < bits) v |= uint64_t(1) << i;
+            push64(b, v);
+        }
     }
     align(b, 4);
     for (uint32_t L = 0; L < m.n; ++L) {
@@ -379,9 +381,8 @@ void build_device_tables(const PuzzleModel& m, const std::vector<LevelPlan>& pla
         // facing colour of the neighbour at side s sits at bits 5*((s+2)&3) of its stack word
         const uint32_t shift_a = arity > 0 ? 5 * ((lp.side[0] + 2u) & 3u) : 0u;
         const uint32_t shift_b = arity > 1 ? 5 * ((lp.side[1] + 2u) & 3u) : 0u;
-        const uint32_t row = t.kw[k] + 2;  // words per pair-table row
-        const uint32_t stride_b = arity > 1 ? row : 0u;
-        const uint32_t stride_a = arity > 1 ? row * t.ncol : (arity > 0 ? row : 0u);
+        const uint32_t stride_b = arity > 1 ? 2 * t.kw[k] : 0u;
+        const uint32_t stride_a = arity > 1 ? 2 * t.kw[k] * t.ncol : (arity > 0 ? 2 * t.kw[k] : 0u);
         d[0] = t.kw[k] | (k << 8) | (nextra << 13) | (t.aoff[k] << 16);
         d[1] = (arity > 0 ? lp.nb_level[0] : 0u) | ((arity > 1 ? lp.nb_level[1] : 0u) << 8) | (shift_a << 16) |
                (shift_b << 24);
@@ -397,7 +398,7 @@ void build_device_tables(const PuzzleModel& m, const std::vector<LevelPlan>& pla
             d[8 + j] = t.tinfo_off[plan[lev].kind];
         }
     }
-    b[0] = 0x454D5033u;  // "EMP3": 32-bit candidate words
+    b[0] = 0x454D5034u;  // "EMP4": 64-bit candidate words, 16-word descriptors
     b[1] = t.n;
     b[2] = t.ncol;
     for (uint32_t k = 0; k < 3; ++k) {

@@ -20,9 +20,11 @@
 //    neighbours & availability;
 //  * a level plan for a position order (row-major "basic" or spiral).
 //
-// Candidate bit t = (kind_index << 2) | orientation, one nibble per piece, in
-// 32-bit words (word t >> 5, bit t & 31: 8 pieces per word), on the host and in
-// the device tables alike.
+// Candidate bit t = (kind_index << 2) | orientation, one nibble per piece.  The
+// host model keeps 32-bit words (word t >> 5, bit t & 31: 8 pieces per word); the
+// device tables (DeviceTables below) store the same bits in 64-bit words (word
+// t >> 6, bit t & 63: 16 pieces per word), so a kernel covers a level's candidate
+// set in few, fully unrolled word operations.
 #pragma once
 
 #include "emp_layout.h"
@@ -78,13 +80,13 @@ struct LevelPlan {
 };
 
 // Flattened tables consumed by the GPU kernels (one blob per puzzle), 32-bit
-// words; the blob size is a multiple of 4 words so blobs can be concatenated
-// keeping 16-byte alignment.
+// words; every 64-bit table starts on an even word and the blob size is a
+// multiple of 4 words so blobs can be concatenated keeping 16-byte alignment.
 //
 // header (kHeaderWords words):
-//   0 magic, 1 n, 2 ncol (= border_id + 1), 3..5 kw[k] (32-bit words per kind),
-//   6..8 aoff[k] (word offset of kind k in the availability array),
-//   9 avail words, 10..12 side[k], 13 pair section, 14 desc,
+//   0 magic, 1 n, 2 ncol (= border_id + 1), 3..5 kw[k] (64-bit words per kind),
+//   6..8 aoff[k] (64-bit word offset of kind k in the availability array),
+//   9 avail words (64-bit), 10..12 side[k], 13 pair section, 14 desc,
 //   15..17 tinfo[k], 18..20 extra[k], 21 initial availability, 22 width,
 //   23 height, 24 blob words, 25 max kw, 26 words of the hot prefix
 // sections in order: header, pair tables, desc, tinfo, side, extra, initial
@@ -94,27 +96,24 @@ struct LevelPlan {
 //   d0 kw | kind<<8 | nextra<<13 | aoff<<16
 //   d1 levelA | levelB<<8 | shiftA<<16 | shiftB<<24 (bit offset of the
 //      neighbour's facing colour in its stack word)
-//   d2 pair table (word offset): rows [cA][cB] (2 placed), [cA] (1), one row (0);
-//      a row is a list header (u16 offset of its candidate list | length << 22),
-//      an occupancy word (bit w set when word w is not zero) and kw words =
-//      frame-side masks & allowed orientations & placed-side masks; the candidate
-//      lists (the row's set bits in ascending order, u16) follow the pair tables
+//   d2 pair table (word offset): rows [cA][cB][kw] (2 placed), [cA][kw] (1), [kw] (0);
+//      entries = frame-side masks & allowed orientations & placed-side masks
 //   d3 strideA | strideB<<16 (words per colour step of A and B; 0 when absent)
 //   d4 side[kind], d5 tinfo[kind], d6 extra[kind],
 //   d7 extra placed sides: side3 | side4<<2 | level3<<8 | level4<<16
 //   d8..d11 tinfo[kind] of the levels of neighbours A, B, 3 and 4 (level 0's kind
 //      when absent), for a stack that keeps transitions without their colours
 //   d12..d15 0
-// side[k]: [side][colour][kw[k]] masks (colour ncol-1 = frame)
+// side[k]: 64-bit [side][colour][kw[k]] masks (colour ncol-1 = frame)
 // tinfo[k]: per transition t, colours of the oriented piece (5 bits per side)
 //           | has_extra<<20 (its identical mask clears other candidates)
-// extra[k]: [4*nk][kw[k]] identical masks
+// extra[k]: 64-bit [4*nk][kw[k]] identical masks
 struct DeviceTables {
     std::vector<uint32_t> blob;
     uint32_t n = 0, ncol = 0, max_kw = 0;
-    std::array<uint32_t, 3> kw{};       // 32-bit words per kind
-    std::array<uint32_t, 3> aoff{};     // availability offset of each kind (words)
-    uint32_t avail_words = 0;           // words
+    std::array<uint32_t, 3> kw{};       // 64-bit words per kind
+    std::array<uint32_t, 3> aoff{};     // availability offset of each kind (64-bit words)
+    uint32_t avail_words = 0;           // 64-bit words
     std::array<uint32_t, 3> side_off{}, tinfo_off{}, extra_off{};
     uint32_t desc_off = 0, pair_off = 0, init_off = 0;
 };

@@ -83,10 +83,10 @@ struct emp_bt_plan_t {
         P.max_levels = max_levels;
         P.max_avail_words = max_avail;
         P.max_kw = max_kw;
-        P.spill = spill.as<uint32_t>();
+        P.spill = spill.as<uint64_t>();
         P.smem_tab_words = smem_tab_words;
         P.rec_words = rec_words;
-        P.rec_r_off = rec_words - max_kw;
+        P.rec_r_off = rec_words - 2 * max_kw;
         P.out_capacity = capacity;
         P.item_budget = budget;
         unsigned long long* c = counters.as<unsigned long long>();

@@ -74,7 +74,7 @@ extern "C" emp_status emp_bt_autotune(const emp_puzzle* puzzles, uint32_t count,
         c.stack_placement = placement;
         consider(c);
     }
-    for (uint32_t threads : {64u, 128u, 256u, 512u}) {
+    for (uint32_t threads : {128u, 256u, 512u}) {
         if (threads == best.threads_per_block) continue;
         emp_bt_config c = best;
         c.threads_per_block = threads;

@@ -254,9 +254,9 @@ class NativePuzzle:
         return list(buf)
 
     def max_kind_words(self) -> int:
-        """32-bit words of the widest kind bitfield (4 bits per piece)."""
+        """64-bit words of the widest kind bitfield (4 bits per piece)."""
         i = self.info()
-        return (4 * max(i.nb_center, i.nb_border, i.nb_corner) + 31) // 32
+        return (4 * max(i.nb_center, i.nb_border, i.nb_corner) + 63) // 64
 
     def table_bytes(self) -> int:
         return 4 * len(self.export_tables())
@@ -521,7 +521,7 @@ class BtPlan:
         """32-bit words per work record (header, prefix, remaining set)."""
         n = max(p.n for p in self.puzzles)
         kw = max(p.max_kind_words() for p in self.puzzles)
-        return 4 + (n + 1) // 2 + kw
+        return 4 + (n + 1) // 2 + 2 * kw
 
     def close(self):
         if getattr(self, "handle", None):

@@ -101,7 +101,7 @@ emp_status emp_puzzle_export_tables(emp_puzzle puzzle, uint32_t *out, uint64_t c
 
 typedef struct emp_bt_config {
     uint32_t split_depth;        /* levels expanded before subtrees go to threads; 0 = auto */
-    uint32_t threads_per_block;  /* 64, 128, 256 or 512; 0 = the size with the most resident warps */
+    uint32_t threads_per_block;  /* 128, 256 or 512; 0 = the size with the most resident warps */
     uint32_t blocks_per_sm;      /* 0 = as many as fit */
     uint32_t stop_at_first;      /* 1: stop once the reference's first solution is known */
     uint64_t reserved_budget;    /* unused, keep 0 */
@@ -261,7 +261,7 @@ typedef struct emp_bt_tune_result {
  * device.  Starting from base (NULL = defaults), it tunes one field at a time, keeping
  * each field's fastest value before moving on:
  *   stack_placement     the DFS stack in shared memory (32- or 16-bit entries) or global memory
- *   threads_per_block   64, 128, 256, 512
+ *   threads_per_block   128, 256, 512
  *   split_subtrees      per-puzzle split targets (batches of several puzzles) or
  *   split_depth         split depths (a single puzzle)
  *   split_budget        steps before a thread hands work back

@@ -72,15 +72,13 @@ def _decode(blob):
                 desc=hdr[14], tinfo=hdr[15:18], extra=hdr[18:21], init=hdr[21], w=hdr[22], h=hdr[23])
 
 
-def _words(blob, off, count):
-    return [blob[off + i] for i in range(count)]
+def _u64(blob, off, count):
+    return [blob[off + 2 * i] | (blob[off + 2 * i + 1] << 32) for i in range(count)]
 
 
 def _candidates_from_tables(blob, h, level, neighbour_colours, order, w):
     """Decodes a level descriptor and returns (kind, candidate bits, placed sides):
-    pair-table row for the first two placed neighbours & side masks of the others.
-    A row is a candidate-list header, an occupancy word (bit w: word w is not zero) and
-    kw 32-bit words."""
+    pair-table row for the first two placed neighbours & side masks of the others."""
     d = blob[h["desc"] + 16 * level: h["desc"] + 16 * level + 16]
     kind, kw, nextra = (d[0] >> 8) & 3, d[0] & 0xFF, (d[0] >> 13) & 7
     pos = order[level]
@@ -103,18 +101,13 @@ def _candidates_from_tables(blob, h, level, neighbour_colours, order, w):
         sides.append(sb)
         assert d[1] >> 24 == 5 * ((sb + 2) % 4)
         row += neighbour_colours[sb] * stride_b
-    words = _words(blob, row + 2, kw)
-    assert blob[row + 1] == sum(1 << i for i, v in enumerate(words) if v)
-    # the row's candidate list: its set bits in ascending order (u16 entries)
-    off, length = blob[row] & 0x3FFFFF, blob[row] >> 22
-    listed = [(blob[(off + i) >> 1] >> (16 * ((off + i) & 1))) & 0xFFFF for i in range(length)]
-    assert listed == [32 * i + b for i, v in enumerate(words) for b in range(32) if (v >> b) & 1]
+    words = _u64(blob, row, kw)
     for j in range(nextra):
         sd = (d[7] >> (2 * j)) & 3
         sides.append(sd)
-        off = d[4] + (sd * h["ncol"] + neighbour_colours[sd]) * kw
-        words = [a & b for a, b in zip(words, _words(blob, off, kw))]
-    return kind, sum(v << (32 * i) for i, v in enumerate(words)), sides
+        off = d[4] + (sd * h["ncol"] + neighbour_colours[sd]) * kw * 2
+        words = [a & b for a, b in zip(words, _u64(blob, off, kw))]
+    return kind, sum(v << (64 * i) for i, v in enumerate(words)), sides
 
 
 @pytest.mark.parametrize("seed", [0, 1, 2, 3])
@@ -170,5 +163,5 @@ def test_identical_masks_match_oracle(seed):
         for t in range(bits):
             m64 = op.identical_mask(kind, t)
             m = sum(v << (64 * i) for i, v in enumerate(m64)) & ((1 << bits) - 1)
-            got = sum(v << (32 * i) for i, v in enumerate(_words(blob, hd["extra"][kind] + t * kw, kw)))
+            got = sum(v << (64 * i) for i, v in enumerate(_u64(blob, hd["extra"][kind] + t * kw * 2, kw)))
             assert got & ((1 << bits) - 1) == m
