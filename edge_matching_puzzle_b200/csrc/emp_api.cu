@@ -435,7 +435,7 @@ emp_status create_plan(const emp_puzzle* puzzles, uint32_t count, const emp_bt_c
     if (pl->max_kw > 16) return fail(EMP_ERR_UNSUPPORTED, "puzzle kinds wider than 16 64-bit words");
     if (pl->cfg.stack_placement > 3)
         return fail(EMP_ERR_INVALID, "stack_placement must be 0 (default), 1, 2 or 3");
-    pl->stack_mode = pl->cfg.stack_placement ? static_cast<int>(pl->cfg.stack_placement) : emp::kStackShared16;
+    pl->stack_mode = pl->cfg.stack_placement ? static_cast<int>(pl->cfg.stack_placement) : emp::kStackShared32;
     std::vector<uint32_t> candidates;
     if (pl->cfg.threads_per_block) candidates.push_back(pl->cfg.threads_per_block);
     else candidates = {128, 256, 512};

@@ -25,7 +25,7 @@ struct emp_bt_plan_t {
     DeviceBuffer counters;                    // [0] cursor, [1] output tail
     DeviceBuffer totals, first_item, records, flags, item_nodes, item_sols, spill, prefix_out;
     DeviceBuffer stack;                       // kStackGlobal32: the threads' DFS stacks
-    int stack_mode = emp::kStackShared16;
+    int stack_mode = emp::kStackShared32;
     DeviceBuffer ctl, incomplete, puzzle_depth_dev;
     std::vector<uint32_t> puzzle_depth;       // per puzzle split depth
     bool adaptive = false;                    // per puzzle split depths (split_subtrees)

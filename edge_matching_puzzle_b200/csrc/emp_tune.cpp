@@ -69,7 +69,7 @@ extern "C" emp_status emp_bt_autotune(const emp_puzzle* puzzles, uint32_t count,
         }
     };
     for (uint32_t placement : {1u, 2u, 3u}) {  // the DFS stack: shared 32-bit, shared 16-bit, global
-        if (placement == (best.stack_placement ? best.stack_placement : 2u)) continue;
+        if (placement == (best.stack_placement ? best.stack_placement : 1u)) continue;
         emp_bt_config c = best;
         c.stack_placement = placement;
         consider(c);
