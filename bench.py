@@ -780,8 +780,14 @@ def main():
             "roofline_onchip": {
                 "kernel": "dfs_kernel", "launch_ms": launch_ms, "placements_per_launch": placements_per_launch,
                 "int_ops_per_placement": ops, "smem_bytes_per_placement": byts, "node_mix_center_border_corner": mix,
+                # integer instructions issue on the ALU pipe (logic, shifts, compares: ncu's
+                # sm__inst_executed_pipe_alu.avg.peak_sustained = 2 warp instructions per SM
+                # cycle, 64 lanes) and on the FMA pipe (integer multiply-add); the issue peak
+                # is 4 schedulers x 32 lanes per SM cycle
                 "int_issue": {"achieved_tops": placements_per_launch * ops / (launch_ms / 1000) / 1e12,
-                              "peak_tops": 148 * 4 * 32 * sm_clock * 1e6 / 1e12},
+                              "peak_tops": 148 * 4 * 32 * sm_clock * 1e6 / 1e12,
+                              "peak_source": "148 SMs x 4 schedulers x 32 lanes x max SM clock (issue slots)",
+                              "alu_pipe_peak_tops": 148 * 2 * 32 * sm_clock * 1e6 / 1e12},
                 "smem": {"achieved_gbs": placements_per_launch * byts / (launch_ms / 1000) / 1e9,
                          "peak_gbs": 148 * 128 * sm_clock * 1e6 / 1e9},
             },
@@ -795,6 +801,7 @@ def main():
         }
         oc = out["roofline_onchip"]
         oc["int_issue"]["frac"] = oc["int_issue"]["achieved_tops"] / oc["int_issue"]["peak_tops"]
+        oc["int_issue"]["alu_pipe_frac"] = oc["int_issue"]["achieved_tops"] / oc["int_issue"]["alu_pipe_peak_tops"]
         oc["smem"]["frac"] = oc["smem"]["achieved_gbs"] / oc["smem"]["peak_gbs"]
         print(json.dumps(out), flush=True)
     for pl in plans:
