@@ -46,7 +46,8 @@ WORKLOAD = (f"exhaustive row-major count of 16 seeded {WIDTH}x{HEIGHT} puzzles (
             f"colours, seeds 0..15), split depth {DEPTH}, one step = 1/{SLICES} slice of the depth-{DEPTH} subtrees")
 L2_BYTES = 126 * 1024 * 1024
 # DRAM bytes (read + write) of one dfs_kernel round on this workload, from one ncu capture
-DFS_LAUNCH_DRAM_BYTES = 172.6e6
+# (dfs_kernel<3, shared tables, 256 threads, shared 32-bit stack>, round 4 of the seed-0 slice)
+DFS_LAUNCH_DRAM_BYTES = 181.3e6
 
 
 def env_int(name, default):
