@@ -18,6 +18,10 @@ restatement of emp_strategy (oracle/emp_oracle.c, checked against the reference'
 search built from its sources in oracle/_ref) on all host cores over a bounded sample
 of the same subtrees: the reference's search is single-threaded and has no way to
 search one subtree, so the multi-threaded restatement is the CPU path timed.
+
+On one GPU the default line also carries ttfs (time to a first solution, plain order
+against the learned order) and glutton (a 10 s glutton max search of the 16x16 puzzle:
+placements/s, levels/s, best level, and the rate in the reference's trial unit).
 """
 from __future__ import annotations
 
@@ -338,6 +342,41 @@ GM_WORKLOAD = (f"glutton max search of the seeded {GM_SIDE}x{GM_SIDE} puzzle ({G
                f"placements")
 
 
+def glutton_reference_unit(native, handle, device):
+    """The GPU's unit is its own trial count: validity passes over the whole level, which
+    evaluate more candidates than the reference's in-place sweep on the same trajectory.
+    The first pushes of the same search, whose reference-unit count the oracle recorded
+    (tests/golden/glutton_16x16.json), give the rate in that unit."""
+    golden = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tests", "golden", "glutton_16x16.json")
+    if not os.path.exists(golden):
+        return None
+    with open(golden) as f:
+        grec = json.load(f)["records"][-1]
+    gr = native.glutton_max(handle, push_budget=grec["push_budget"], device=device)
+    if gr.pushes != grec["pushes"] or gr.max_level != grec["max_level"]:
+        return None
+    return {"pushes": grec["pushes"], "oracle_placements": grec["placements"],
+            "gpu_trials_plus_pushes": gr.trials + gr.pushes, "gpu_ms": gr.kernel_ms,
+            "placements_per_s": grec["placements"] / (gr.kernel_ms / 1000.0),
+            "gpu_per_reference_unit": (gr.trials + gr.pushes) / grec["placements"]}
+
+
+def glutton_leg(local_rank):
+    """One time-bounded glutton max search of the 16x16 puzzle for the default line."""
+    from edge_matching_puzzle_b200 import native
+    from edge_matching_puzzle_b200.puzzle import generate
+    pz = generate(GM_SIDE, GM_SIDE, GM_BORDER, GM_INTERIOR, GM_SEED)
+    handle = native.NativePuzzle(pz.width, pz.height, pz.colors)
+    native.glutton_max(handle, push_budget=1, device=local_rank)  # warm-up
+    r = native.glutton_max(handle, timeout_ms=GM_STEP_MS, device=local_rank)
+    sec = r.kernel_ms / 1000.0
+    out = {"workload": GM_WORKLOAD.replace("one step = ", "one search: "), "placements_per_s": (r.trials + r.pushes) / sec,
+           "levels_per_s": r.levels / sec, "best_level": r.max_level, "search_s": sec, "pushes": r.pushes,
+           "pops": r.pops, "reference_unit": glutton_reference_unit(native, handle, local_rank)}
+    handle.close()
+    return out
+
+
 def run_glutton(args, rank, world, local_rank):
     """Greedy max-placement search of the 16x16 puzzle: placements/s of one search."""
     import torch
@@ -384,21 +423,7 @@ def run_glutton(args, rank, world, local_rank):
     value = placements / sec
     n = GM_SIDE * GM_SIDE
     peak_sm = 4 * 32 * ((clocks or {}).get("sm_max_mhz") or 1965.0) * 1e6  # lane-ops/s of one SM
-    # The GPU's unit is its own trial count: validity passes over the whole level, which
-    # evaluate more candidates than the reference's in-place sweep on the same
-    # trajectory.  The first pushes of the same search, whose reference-unit count the
-    # oracle recorded (tests/golden/glutton_16x16.json), give the rate in that unit.
-    ref_unit = None
-    golden = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tests", "golden", "glutton_16x16.json")
-    if os.path.exists(golden):
-        with open(golden) as f:
-            grec = json.load(f)["records"][-1]
-        gr = native.glutton_max(handle, push_budget=grec["push_budget"], device=local_rank)
-        if gr.pushes == grec["pushes"] and gr.max_level == grec["max_level"]:
-            ref_unit = {"pushes": grec["pushes"], "oracle_placements": grec["placements"],
-                        "gpu_trials_plus_pushes": gr.trials + gr.pushes, "gpu_ms": gr.kernel_ms,
-                        "placements_per_s": grec["placements"] / (gr.kernel_ms / 1000.0),
-                        "gpu_per_reference_unit": (gr.trials + gr.pushes) / grec["placements"]}
+    ref_unit = glutton_reference_unit(native, handle, local_rank)
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1000 * sec / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -558,8 +583,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
     ap.add_argument("--no-ttfs", action="store_true", help="skip the time-to-first-solution leg (plain vs learned)")
+    ap.add_argument("--no-glutton", action="store_true", help="skip the 10 s glutton max leg of the default line")
     ap.add_argument("--stack-placement", type=int, default=0,
-                    help="DFS stack: 0 library default, 1 shared 32-bit, 2 shared 16-bit, 3 global memory")
+                    help="DFS stack: 0 library default, 1 shared 32-bit, 2 shared 16-bit, 3 global memory, 4 one DFS per warp")
     ap.add_argument("--host-loop", action="store_true",
                     help="launch each DFS round from the host, one puzzle after another (the default runs each "
                          "puzzle's rounds as one CUDA graph, puzzles on concurrent streams)")
@@ -738,6 +764,9 @@ def main():
     if rank == 0 and world == 1 and not args.no_ttfs:
         ttfs = ttfs_measure(local_rank, TTFS_TRAIN_SEEDS, TTFS_EVAL_SEEDS, args.learn_epochs, TTFS_TIMEOUT_MS)
         ttfs["workload"] = TTFS_WORKLOAD
+    glutton = None
+    if rank == 0 and world == 1 and not args.no_glutton:
+        glutton = glutton_leg(local_rank)
 
     # ---------------- CPU baseline (oracle) and algorithmic work ----------------
     peaks, peak_kind = measured_peaks()
@@ -796,6 +825,7 @@ def main():
             "e2e": e2e,
             "cpu_baseline": cpu,
             "ttfs": ttfs,
+            "glutton": glutton,
             "dfs": {"rounds_per_step": rounds / args.steps, "launch": "host loop" if not graphs else
                     "one CUDA graph per puzzle slice (device-side round loop), 16 concurrent streams",
                     "busy_frac": busy / ms if ms and not graphs else None},

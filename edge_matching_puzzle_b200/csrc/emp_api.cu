@@ -432,10 +432,16 @@ emp_status create_plan(const emp_puzzle* puzzles, uint32_t count, const emp_bt_c
     // launch geometry: the block size with the most resident warps per SM
     cudaDeviceProp prop;
     CUDA_TRY(cudaGetDeviceProperties(&prop, pl->device));
-    if (pl->max_kw > 16) return fail(EMP_ERR_UNSUPPORTED, "puzzle kinds wider than 16 64-bit words");
-    if (pl->cfg.stack_placement > 3)
-        return fail(EMP_ERR_INVALID, "stack_placement must be 0 (default), 1, 2 or 3");
-    pl->stack_mode = pl->cfg.stack_placement ? static_cast<int>(pl->cfg.stack_placement) : emp::kStackShared32;
+    if (pl->cfg.stack_placement > 4)
+        return fail(EMP_ERR_INVALID, "stack_placement must be 0 (default), 1, 2, 3 or 4");
+    // default: shared memory next to staged tables (a single puzzle); for a batch, whose
+    // tables stay in global memory, the global stack measured faster (more warps per SM)
+    pl->stack_mode = pl->cfg.stack_placement ? static_cast<int>(pl->cfg.stack_placement)
+                                             : (pl->smem_tab_words ? emp::kStackShared32 : emp::kStackGlobal32);
+    if (pl->stack_mode == emp::kStackWarp ? pl->max_kw > 32 : pl->max_kw > 16)
+        return fail(EMP_ERR_UNSUPPORTED, pl->stack_mode == emp::kStackWarp
+                                             ? "puzzle kinds wider than 32 64-bit words"
+                                             : "puzzle kinds wider than 16 64-bit words (stack_placement 4 takes 32)");
     std::vector<uint32_t> candidates;
     if (pl->cfg.threads_per_block) candidates.push_back(pl->cfg.threads_per_block);
     else candidates = {128, 256, 512};

@@ -783,6 +783,385 @@ __global__ void __launch_bounds__(T) dfs_kernel(BtLaunch P)
     }
 }
 
+// ---------------------------------------------------------------------------
+// Warp-cooperative DFS (stack placement kStackWarp): one record per warp.  The
+// warp's stack (32-bit entries as above) sits in shared memory; lane w holds
+// word w of each kind's availability in registers and evaluates candidate word
+// w of a level, so a try is one ballot over the words and one find-first-set
+// in the first non-empty lane (the reference's warp method,
+// src/CUDA_backtracker.cu:86-120, over the exhaustive search's candidate sets).
+// Kinds up to 32 words (2048 transitions).  Every branch below is warp-uniform:
+// the state `s` is the same in all lanes, and values read from memory that
+// other warps change (the queue cursor, flags, first-solution records, the
+// clock) are taken from lane 0.
+
+struct WarpAv {
+    uint64_t k0 = 0, k1 = 0, k2 = 0;  // word `lane` of kinds 0, 1, 2
+    __device__ __forceinline__ uint64_t get(uint32_t kind) const { return kind == 0 ? k0 : (kind == 1 ? k1 : k2); }
+    __device__ __forceinline__ void flip(uint32_t kind, uint64_t nib, bool give_back)
+    {
+        // selects, not a reference to the chosen member, so the words stay in registers
+        const uint64_t m0 = kind == 0 ? nib : 0ull, m1 = kind == 1 ? nib : 0ull, m2 = kind == 2 ? nib : 0ull;
+        if (give_back) {
+            k0 |= m0;
+            k1 |= m1;
+            k2 |= m2;
+        } else {
+            k0 &= ~m0;
+            k1 &= ~m1;
+            k2 &= ~m2;
+        }
+    }
+};
+
+using WarpStk = Stk<kStackShared32, 1>;
+
+// this lane's candidate word of level l (not masked by the resume bit)
+template <bool SM>
+__device__ __forceinline__ uint64_t warp_candidates(const BtLaunch& P, const ThreadItem& s, const LevelDesc& d,
+                                                    uint32_t l, bool spilled, const WarpStk& stk, const WarpAv& av,
+                                                    const uint64_t* spill, uint32_t lane)
+{
+    const uint32_t kw = d.kw();
+    if (lane >= kw) return 0ull;
+    if (spilled) return spill[l * P.max_kw + lane];
+    const uint32_t ca = stk.template colour<SM>(s, d.level_a(), d.shift_a(), 0u);
+    const uint32_t cb = stk.template colour<SM>(s, d.level_b(), d.shift_b(), 0u);
+    uint64_t x = Tab<SM>::u64(s, d.d2 + ca * d.stride_a() + cb * d.stride_b() + 2 * lane) & av.get(d.kind());
+    if (d.nextra()) {
+        const uint32_t ncol = Tab<SM>::u32(s, H_NCOL);
+        for (uint32_t j = 0; j < d.nextra(); ++j) {
+            const uint32_t sd = d.extra_side(j);
+            const uint32_t c = stk.template colour<SM>(s, d.extra_level(j), 5 * ((sd + 2) & 3u), 0u);
+            x &= ldg64(s.tb + d.d4 + ((sd * ncol + c) * kw) * 2 + 2 * lane);
+        }
+    }
+    return x;
+}
+
+__device__ __forceinline__ uint64_t from_bit(uint32_t start, uint32_t lane)
+{
+    const int sh = static_cast<int>(start) - 64 * static_cast<int>(lane);
+    return shl_sat(~0ull, static_cast<uint32_t>(sh > 0 ? sh : 0));
+}
+
+template <bool SM>
+__device__ __forceinline__ void warp_load_record(const BtLaunch& P, ThreadItem& s, const uint32_t* rec, WarpStk& stk,
+                                                 WarpAv& av, uint64_t* spill, uint32_t lane)
+{
+    using TB = Tab<SM>;
+    s.orig = static_cast<uint64_t>(rec[0]) | (static_cast<uint64_t>(rec[1]) << 32);
+    const uint32_t len = rec[2] & 0xFFFFu;
+    s.start = rec[2] >> 16;
+    s.pz = rec[3] & 0xFFFFu;
+    s.spilled = (rec[3] >> 16) & 1u;
+    s.tb = P.tables + P.puzzle_offset[s.pz];
+    s.n = TB::u32(s, H_N);
+    s.desc_off = TB::u32(s, H_DESC);
+    const uint32_t init = TB::u32(s, H_INIT);
+    uint64_t w[3];
+#pragma unroll
+    for (uint32_t k = 0; k < 3; ++k)
+        w[k] = lane < TB::u32(s, H_KW + k) ? ldg64(s.tb + init + 2 * (TB::u32(s, H_AOFF + k) + lane)) : 0ull;
+    av.k0 = w[0];
+    av.k1 = w[1];
+    av.k2 = w[2];
+    for (uint32_t l = 0; l < len; ++l) {
+        const uint32_t kind = (TB::u32(s, s.desc_off + kDescWords * l) >> 8) & 3u;
+        const uint32_t t = rec_t(rec, l);
+        if (lane == (t >> 6)) av.flip(kind, 0xFull << (t & 60u), false);
+    }
+    for (uint32_t l = lane; l < len; l += 32) {
+        const uint32_t t = rec_t(rec, l);
+        stk.put(l, t, false, 0u, TB::u32(s, TB::u32(s, s.desc_off + kDescWords * l + 5) + t));
+    }
+    if (s.spilled && lane < P.max_kw) {
+        const uint32_t* R = rec + P.rec_r_off;
+        spill[len * P.max_kw + lane] =
+            static_cast<uint64_t>(R[2 * lane]) | (static_cast<uint64_t>(R[2 * lane + 1]) << 32);
+    }
+    __syncwarp();
+    s.L = len;
+    s.base = len;
+    s.pop = false;
+    s.nodes = 0;
+    s.sols = 0;
+    s.steps = 0;
+    s.active = true;
+}
+
+// One step of emp_strategy::specific_run (include/emp_strategy.h:352-401) by the
+// whole warp: go up one level when the current one is exhausted, then place the
+// next candidate of the current level (a dead end marks the level exhausted for
+// the next step).  Returns false once the record is exhausted.
+template <bool SM>
+__device__ __forceinline__ bool warp_step(const BtLaunch& P, ThreadItem& s, WarpStk& stk, WarpAv& av,
+                                          uint64_t* spill, uint32_t lane, bool* solved)
+{
+    if (s.pop) {
+        if (s.L == s.base) return false;
+        --s.L;
+        const uint32_t t = stk.t(s.L);
+        s.spilled = stk.spilled(s.L);
+        s.pop = !stk.more(s.L);
+        const uint32_t kind = (Tab<SM>::u32(s, s.desc_off + kDescWords * s.L) >> 8) & 3u;
+        if (lane == (t >> 6)) av.flip(kind, 0xFull << (t & 60u), true);
+        s.start = t + 1;
+        if (s.pop) return true;
+    }
+    const LevelDesc d = Tab<SM>::desc(s, s.L, false);
+    const uint64_t xu = warp_candidates<SM>(P, s, d, s.L, s.spilled != 0, stk, av, spill, lane);
+    const uint64_t x = xu & from_bit(s.start, lane);
+    const unsigned bal = __ballot_sync(kFull, x != 0ull);
+    if (!bal) {
+        s.pop = true;  // dead end: go up at the next step
+        return true;
+    }
+    const uint32_t fw = __ffs(bal) - 1;
+    const uint64_t xf = __shfl_sync(kFull, x, fw);
+    const uint32_t t = fw * 64 + __ffsll(xf) - 1;
+    const unsigned after = fw < 31 ? bal >> (fw + 1) : 0u;
+    bool more = (xf & (xf - 1)) != 0ull || after != 0u;
+    const uint32_t ti = Tab<SM>::u32(s, d.d5 + t);
+    if ((ti >> 20) & 1u) {
+        // select_piece with an identical mask (emp_position_strategy.h:197-200): the
+        // level keeps its exact remaining set from now on
+        const uint32_t kw = d.kw();
+        uint64_t sp = 0;
+        if (lane < kw) {
+            sp = (s.spilled ? x : xu) & ldg64(s.tb + d.d6 + t * kw * 2 + 2 * lane);
+            spill[s.L * P.max_kw + lane] = sp;
+        }
+        more = __ballot_sync(kFull, (sp & from_bit(t + 1, lane)) != 0ull) != 0u;
+        s.spilled = 1;
+    }
+    const uint32_t kind = d.kind();
+    const uint64_t nib = 0xFull << (t & 60u);
+    if (lane == (t >> 6)) av.flip(kind, nib, false);
+    if (lane == 0) stk.put(s.L, t, more, s.spilled, ti);
+    __syncwarp();
+    ++s.nodes;
+    if (s.L == s.n - 1) {
+        // solution: count it, give the piece back, try the next candidate
+        ++s.sols;
+        *solved = true;
+        if (lane == (t >> 6)) av.flip(kind, nib, true);
+        s.start = t + 1;
+        s.pop = !more;
+    } else {
+        ++s.L;
+        s.start = 0;
+        s.spilled = 0;
+    }
+    return true;
+}
+
+// split_record for a warp: the same records, written by the lanes together
+template <bool SM>
+__device__ __forceinline__ bool warp_level_has_work(const BtLaunch& P, const ThreadItem& s, uint32_t l,
+                                                    const WarpStk& stk, const WarpAv& av, const uint64_t* spill,
+                                                    uint32_t lane, uint32_t* start_out, uint32_t* spilled_out)
+{
+    uint32_t start, spilled;
+    bool maybe;
+    if (l == s.L) {
+        start = s.start;
+        spilled = s.spilled;
+        maybe = !s.pop;
+    } else {
+        start = stk.t(l) + 1;
+        spilled = stk.spilled(l);
+        maybe = stk.more(l);
+    }
+    *start_out = start;
+    *spilled_out = spilled;
+    if (!maybe) return false;
+    const LevelDesc d = Tab<SM>::desc(s, l, false);
+    const uint64_t x = warp_candidates<SM>(P, s, d, l, spilled != 0, stk, av, spill, lane) & from_bit(start, lane);
+    return __ballot_sync(kFull, x != 0ull) != 0u;
+}
+
+template <bool SM>
+__device__ __forceinline__ void warp_toggle_piece(const ThreadItem& s, uint32_t l, const WarpStk& stk, WarpAv& av,
+                                                  uint32_t lane, bool give_back)
+{
+    const uint32_t kind = (Tab<SM>::u32(s, s.desc_off + kDescWords * l) >> 8) & 3u;
+    const uint32_t t = stk.t(l);
+    if (lane == (t >> 6)) av.flip(kind, 0xFull << (t & 60u), give_back);
+}
+
+template <bool SM>
+__device__ bool warp_split_record(const BtLaunch& P, ThreadItem& s, const WarpStk& stk, WarpAv& av,
+                                  const uint64_t* spill, uint32_t lane)
+{
+    uint32_t cnt = 0, start, spilled;
+    for (uint32_t l = s.L + 1; l-- > s.base;) {
+        if (l < s.L) warp_toggle_piece<SM>(s, l, stk, av, lane, true);
+        cnt += warp_level_has_work<SM>(P, s, l, stk, av, spill, lane, &start, &spilled);
+    }
+    unsigned long long slot = 0;
+    if (lane == 0 && cnt) slot = atomicAdd(P.out_tail, (unsigned long long)cnt);
+    slot = __shfl_sync(kFull, slot, 0);
+    const bool fits = slot + cnt <= P.out_capacity;
+    unsigned long long k = slot;
+    for (uint32_t l = s.base; l <= s.L; ++l) {
+        if (warp_level_has_work<SM>(P, s, l, stk, av, spill, lane, &start, &spilled)) {
+            if (fits) {
+                uint32_t* rec = P.out_rec + k * P.rec_words;
+                if (lane == 0) {
+                    rec[0] = static_cast<uint32_t>(s.orig);
+                    rec[1] = static_cast<uint32_t>(s.orig >> 32);
+                    rec[2] = l | (start << 16);
+                    rec[3] = s.pz | (spilled << 16);
+                }
+                for (uint32_t j = 2 * lane; j < l; j += 64) {
+                    const uint32_t lo = stk.t(j);
+                    const uint32_t hi = j + 1 < l ? stk.t(j + 1) : 0u;
+                    rec[4 + (j >> 1)] = lo | (hi << 16);
+                }
+                if (spilled && lane < P.max_kw) {
+                    const uint64_t v = spill[l * P.max_kw + lane];
+                    rec[P.rec_r_off + 2 * lane] = static_cast<uint32_t>(v);
+                    rec[P.rec_r_off + 2 * lane + 1] = static_cast<uint32_t>(v >> 32);
+                }
+            } else if (k < P.out_capacity && lane == 0) {
+                P.out_rec[k * P.rec_words + 3] = 1u << 17;  // reserved slot that fits: mark empty
+            }
+            ++k;
+        }
+        if (l < s.L) warp_toggle_piece<SM>(s, l, stk, av, lane, false);
+    }
+    return fits;
+}
+
+template <bool SM, int T, int kStepsPerFetch>
+__global__ void __launch_bounds__(T) dfs_warp_kernel(BtLaunch P)
+{
+    const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (SM) {
+        const uint4* src = reinterpret_cast<const uint4*>(P.tables + P.puzzle_offset[0]);
+        uint4* dst = reinterpret_cast<uint4*>(g_smem);
+        for (uint32_t i = tid; i < P.smem_tab_words / 4; i += T) dst[i] = __ldg(src + i);
+        __syncthreads();
+    }
+    WarpStk stk;
+    stk.p = g_smem + P.smem_tab_words + warp * P.max_levels;
+    const uint64_t gwarp = static_cast<uint64_t>(blockIdx.x) * (T / 32) + warp;
+    uint64_t* spill = P.spill + gwarp * P.max_levels * P.max_kw;
+    ThreadItem s;
+    s.active = false;
+    WarpAv av;
+    bool drained = false;
+    uint32_t since_check = 0;
+    const uint64_t deadline = *(volatile unsigned long long*)&P.ctl->deadline;
+    const uint64_t n_in = P.n_in_from_ctl ? *(volatile unsigned long long*)&P.ctl->n_in : P.n_in;
+
+    for (;;) {
+        if (!s.active) {
+            // ---- work fetch: one record per warp ----
+            unsigned long long my = 0;
+            int abort = 0;
+            if (lane == 0) {
+                my = atomicAdd(P.cursor, 1ull);
+                abort = *(volatile int*)P.abort_flag;
+            }
+            my = __shfl_sync(kFull, my, 0);
+            abort = __shfl_sync(kFull, abort, 0);
+            if (my >= n_in) break;
+            drained = my + 1 >= n_in;
+            const uint32_t* rec = P.in_rec + my * P.rec_words;
+            const uint32_t flags = rec[3];
+            if ((flags >> 17) & 1u) continue;  // an empty slot
+            if (abort) {
+                if (lane == 0) P.incomplete[flags & 0xFFFFu] = 1u;  // stopped: the record stays unsearched
+                continue;
+            }
+            warp_load_record<SM>(P, s, rec, stk, av, spill, lane);
+            if (P.stop_at_first) {
+                unsigned long long f = 0;
+                if (lane == 0) f = *(volatile unsigned long long*)&P.first_item[s.pz];
+                if (s.orig > __shfl_sync(kFull, f, 0)) s.active = false;  // a lower subtree holds a solution
+            }
+            continue;
+        }
+        for (int step = 0; step < kStepsPerFetch; ++step) {
+            bool solved = false;
+            if (!warp_step<SM>(P, s, stk, av, spill, lane, &solved)) {
+                if (lane == 0) account(P, s);
+                s.active = false;
+                break;
+            }
+            if (solved) {
+                if (lane == 0) record_solution(P, s, stk);
+                if (P.sols) {
+                    unsigned long long slot = 0;
+                    if (lane == 0) slot = atomicAdd(P.sol_count, 1ull);
+                    slot = __shfl_sync(kFull, slot, 0);
+                    if (slot < P.sol_capacity) {
+                        SolutionRecord* r = P.sols + slot;
+                        if (lane == 0) {
+                            r->orig = s.orig;
+                            r->local = s.nodes;
+                        }
+                        for (uint32_t l = lane; l < s.n; l += 32) r->t[l] = static_cast<uint16_t>(stk.t(l));
+                    }
+                }
+                if (P.stop_at_any && lane == 0) {
+                    atomicCAS(&P.ctl->first_found_ns, 0ull, static_cast<unsigned long long>(global_ns()));
+                    atomicExch(P.abort_flag, 1);
+                }
+                __syncwarp();
+            }
+        }
+        if (!s.active) continue;
+        s.steps += kStepsPerFetch;
+        since_check += kStepsPerFetch;
+
+        // ---- once the queue is empty, hand work back for the next round ----
+        if (!drained && (since_check & 1023u) == 0u) {
+            unsigned long long c = 0;
+            if (lane == 0) c = *(volatile unsigned long long*)P.cursor;
+            drained = __shfl_sync(kFull, c, 0) >= n_in;
+        }
+        if (drained && P.item_budget && s.steps >= P.item_budget) {
+            if (warp_split_record<SM>(P, s, stk, av, spill, lane)) {
+                if (lane == 0) account(P, s);
+                s.active = false;
+                break;  // this warp's work went back to the queue; the queue is empty
+            }
+            s.steps = 0;
+        }
+        // ---- deadline, cancellation and stop-at-first, every 4096 steps ----
+        if (since_check >= 4096) {
+            since_check = 0;
+            int flags = 0;
+            if (lane == 0) {
+                if (*(volatile int*)P.abort_flag != 0) flags |= 1;
+                if (deadline && global_ns() > deadline) flags |= 2;
+                if (P.stop_at_first && s.orig > *(volatile unsigned long long*)&P.first_item[s.pz]) flags |= 4;
+            }
+            flags = __shfl_sync(kFull, flags, 0);
+            const bool stop = (flags & 3) != 0;
+            if (stop || (flags & 4)) {
+                if (lane == 0) {
+                    account(P, s);
+                    if (flags & 2) atomicOr(P.status, EMP_DEV_TIMEOUT);
+                    if (stop) {
+                        // the warp goes on taking records only to mark their puzzles
+                        // incomplete, so every dropped piece of work is known
+                        P.incomplete[s.pz] = 1u;
+                        atomicExch(P.abort_flag, 1);
+                        atomicOr(P.status, EMP_DEV_ABORTED);
+                    } else {
+                        atomicOr(P.status, EMP_DEV_SUPERSEDED);
+                    }
+                }
+                s.active = false;
+            }
+        }
+    }
+}
+
 __global__ void reset_kernel(BtLaunch P, uint32_t n_puzzles)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -935,6 +1314,10 @@ const void* dfs_symbol_mode(uint32_t max_kw, bool sm, int mode)
         case kStackShared32: return dfs_symbol_kw<T, kStackShared32>(max_kw, sm);
         case kStackShared16: return dfs_symbol_kw<T, kStackShared16>(max_kw, sm);
         case kStackGlobal32: return dfs_symbol_kw<T, kStackGlobal32>(max_kw, sm);
+        case kStackWarp:
+            if (max_kw > 32) return nullptr;
+            return sm ? reinterpret_cast<const void*>(&dfs_warp_kernel<true, T, 32>)
+                      : reinterpret_cast<const void*>(&dfs_warp_kernel<false, T, 32>);
         default: return nullptr;
     }
 }
@@ -1014,6 +1397,9 @@ uint64_t scan_block_sum_words(uint64_t n) { return (n + kScanBlock - 1) / kScanB
 size_t dfs_smem_bytes(uint32_t max_levels, uint32_t max_avail_words, uint32_t threads, uint32_t tab_words,
                       int stack_mode)
 {
+    if (stack_mode == kStackWarp)  // one stack per warp; availability in registers
+        return static_cast<size_t>(tab_words) * sizeof(uint32_t) +
+               static_cast<size_t>(threads / 32) * max_levels * sizeof(uint32_t);
     const size_t stack = stack_mode == kStackShared32 ? 4 : (stack_mode == kStackShared16 ? 2 : 0);
     return static_cast<size_t>(tab_words) * sizeof(uint32_t) +
            static_cast<size_t>(max_avail_words) * sizeof(uint64_t) * threads +

@@ -58,6 +58,11 @@ extern "C" emp_status emp_bt_autotune(const emp_puzzle* puzzles, uint32_t count,
     best.stop_at_first = 0;
     Trial t{puzzles, count, trial_ms};
     double best_rate = time_config(t, best);
+    if (best_rate < 0 && !best.stack_placement) {
+        best.stack_placement = 4;  // kinds wider than the per-thread search takes: one DFS per warp
+        best_rate = time_config(t, best);
+        if (best_rate < 0) best.stack_placement = 0;
+    }
     if (best_rate < 0)
         return fail(EMP_ERR_INVALID, "emp_bt_autotune: the base configuration does not run: " + emp::last_error());
     const double default_rate = best_rate;
@@ -68,8 +73,9 @@ extern "C" emp_status emp_bt_autotune(const emp_puzzle* puzzles, uint32_t count,
             best = cand;
         }
     };
-    for (uint32_t placement : {1u, 2u, 3u}) {  // the DFS stack: shared 32-bit, shared 16-bit, global
-        if (placement == (best.stack_placement ? best.stack_placement : 1u)) continue;
+    // the DFS stack: shared 32-bit, shared 16-bit, global, one per warp
+    for (uint32_t placement : {1u, 2u, 3u, 4u}) {
+        if (placement == best.stack_placement) continue;  // 0, the default, is none of them
         emp_bt_config c = best;
         c.stack_placement = placement;
         consider(c);

@@ -130,11 +130,16 @@ typedef struct emp_bt_config {
                                     A wait that runs out reports EMP_FIRST_LOST for the puzzle */
     uint32_t hold_first_lock;    /* testing only: 1 = every first-solution record starts locked by
                                     nobody, so each wait runs out (exercises EMP_FIRST_LOST) */
-    uint32_t stack_placement;    /* where each thread keeps its DFS stack: 0 = default (1),
+    uint32_t stack_placement;    /* where each thread keeps its DFS stack: 0 = default (1 when
+                                    the tables are staged in shared memory, else 3),
                                     1 = shared memory, 32-bit entries with the placed piece's colours,
                                     2 = shared memory, 16-bit entries (more threads per SM; colours are
                                         read from the transition table),
-                                    3 = global memory (L1-cached), 32-bit entries */
+                                    3 = global memory (L1-cached), 32-bit entries,
+                                    4 = one DFS per warp: the warp's stack in shared memory,
+                                        lane w evaluates candidate word w and a ballot picks
+                                        the next candidate (kinds up to 32 words; 1 to 3
+                                        take 16) */
 } emp_bt_config;
 
 typedef struct emp_bt_result {
@@ -260,7 +265,8 @@ typedef struct emp_bt_tune_result {
 /* Chooses the launch parameters for a set of puzzles by timing short runs on the
  * device.  Starting from base (NULL = defaults), it tunes one field at a time, keeping
  * each field's fastest value before moving on:
- *   stack_placement     the DFS stack in shared memory (32- or 16-bit entries) or global memory
+ *   stack_placement     the DFS stack in shared memory (32- or 16-bit entries) or global memory,
+ *                       or one DFS per warp (tried first when the kinds are too wide for the others)
  *   threads_per_block   128, 256, 512
  *   split_subtrees      per-puzzle split targets (batches of several puzzles) or
  *   split_depth         split depths (a single puzzle)

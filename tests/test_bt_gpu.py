@@ -371,10 +371,10 @@ def test_resume_solutions_results_bin_equals_reference_build():
         assert hashlib.sha256(_results_bin(pz, order, sols, res.nodes)).hexdigest() == rec["results_sha256"], rec["name"]
 
 
-@pytest.mark.parametrize("placement", [1, 2, 3])
+@pytest.mark.parametrize("placement", [1, 2, 3, 4])
 def test_stack_placements_equal_reference_build(placement):
-    """Every placement of the DFS stack (shared 32-bit, shared 16-bit, global) gives the
-    reference build's counts, with work handed between threads (small split budget)."""
+    """Every placement of the DFS stack (shared 32-bit, shared 16-bit, global, one DFS per
+    warp) gives the reference build's counts, with work handed back (small split budget)."""
     recs = [r for r in REF_RECORDS if r["group"] in ("config0", "random", "quirk")]
     for rec in recs:
         pz = Puzzle.from_csv(rec["csv"])
@@ -401,3 +401,38 @@ def test_variable_space_debug_mode(reference_vectors, name):
     if reference_vectors["backtracker_trace"][name]:
         assert [f"Thread {l} : selected variable {v} at step {s}" for l, v, s in events] == \
             reference_vectors["backtracker_trace"][name]
+
+
+def test_warp_mode_resume_and_solutions_equal_reference_build():
+    """One DFS per warp (stack_placement 4): resumed counts and the resumed search's
+    results.bin equal the reference build's, with and without work handed back."""
+    from edge_matching_puzzle_b200.puzzle import parse_board_string, situation_transitions
+    for rec in [r for r in REF_RECORDS if r["group"] == "resume"]:
+        pz = Puzzle.from_csv(rec["csv"])
+        order = _ref_order(rec, pz)
+        trans = situation_transitions(pz, order, parse_board_string(pz.width, pz.height, rec["initial_situation"]))
+        npz = native.NativePuzzle(pz.width, pz.height, pz.colors, order=order)
+        for budget in (0, 64):
+            r = native.bt_resume(npz, trans, split_budget=budget, stack_placement=4)
+            assert r.status == native.EMP_OK
+            assert (r.nodes, r.solutions) == (rec["nodes"], rec["solutions"]), rec["name"]
+        if rec["solutions"] <= 4096:
+            found, sols, res = native.bt_resume_solutions(npz, trans, capacity=4096, stack_placement=4)
+            assert found == rec["solutions"] and res.nodes == rec["nodes"], rec["name"]
+            assert hashlib.sha256(_results_bin(pz, order, sols, res.nodes)).hexdigest() == \
+                rec["results_sha256"], rec["name"]
+
+
+@pytest.mark.parametrize("seed", [4, 12])
+def test_warp_mode_8x8_full_count(config_counts, seed):
+    """One DFS per warp on whole 8x8 workload counts (3.8e9 and 1.9e10 placements), with
+    the first solution, against the CPU oracle's counts."""
+    rec = [r for r in config_counts["records"] if r["config"] == "8x8" and r["seed"] == seed][0]
+    pz = generate(8, 8, 4, 8, seed)
+    h = native.NativePuzzle(8, 8, pz.colors)
+    r = native.bt_count(h, split_depth=12, stack_placement=4, timeout_ms=240000)
+    assert r.status == native.EMP_OK
+    assert (r.nodes, r.solutions) == (rec["nodes"], rec["solutions"])
+    ref = native.bt_count(h, split_depth=12)
+    assert bool(r.has_first_solution) == (rec["solutions"] > 0)
+    assert list(r.first_solution)[:64] == list(ref.first_solution)[:64]

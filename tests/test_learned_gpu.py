@@ -114,7 +114,7 @@ def test_ordered_plan_keeps_the_exhaustive_counts():
     m = native.Mlp(seed=3)
     m.train(handles, boards, epochs=5, batch=512)
     for seed in (21, 22):
-        pz = generate(7, 7, 3, 5, seed)
+        pz = generate(7, 7, 3, 6, seed)  # about 3e10 placements each
         h = native.NativePuzzle(7, 7, pz.colors)
         plain = native.BtPlan([h], split_depth=8)
         plain.run()

@@ -64,8 +64,8 @@ def test_noalloc_leaves_free_device_memory_unchanged():
         pytest.skip("no CUDA device visible to torch")
     pz = generate(6, 6, 3, 6, 5)
     handle = native.NativePuzzle(pz.width, pz.height, pz.colors)
-    native.glutton_max_noalloc(handle, timeout_ms=60000)          # set-up on this device
+    native.glutton_max_noalloc(handle, push_budget=200)           # set-up on this device
     before = torch.cuda.mem_get_info()[0]
     for _ in range(3):
-        native.glutton_max_noalloc(handle, timeout_ms=60000)
+        native.glutton_max_noalloc(handle, push_budget=200)
     assert torch.cuda.mem_get_info()[0] == before
