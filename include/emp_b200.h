@@ -131,7 +131,8 @@ typedef struct emp_bt_config {
     uint32_t hold_first_lock;    /* testing only: 1 = every first-solution record starts locked by
                                     nobody, so each wait runs out (exercises EMP_FIRST_LOST) */
     uint32_t stack_placement;    /* where each thread keeps its DFS stack: 0 = default (1 when
-                                    the tables are staged in shared memory, else 3),
+                                    the tables are staged in shared memory and 1 leaves at
+                                    least 16 warps per SM, else 3),
                                     1 = shared memory, 32-bit entries with the placed piece's colours,
                                     2 = shared memory, 16-bit entries (more threads per SM; colours are
                                         read from the transition table),
