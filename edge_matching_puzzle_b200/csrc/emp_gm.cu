@@ -43,6 +43,11 @@ struct GmSmem {
     uint8_t N[256][256];       // N[j][q]: orientations of piece q left at info j
     uint32_t lo[256][6];       // per piece q: six smallest (A[j]-N[j][q]) << 16 | j, ~0 empty
     uint32_t hi[256][6];       // per piece q: six largest (A[j]-N[j][q]+1) << 16 | j, 0 empty
+    uint32_t lo2[256][6];      // the same two lists over the second half of the infos,
+    uint32_t hi2[256][6];      // merged into lo / hi at the end of each statistics pass
+    uint16_t S2[256];
+    uint32_t partA[32];        // per warp: bits of its infos, and whether one is empty
+    uint32_t partE[32];
     uint32_t cc[32][4][32];    // colour constraints
     uint16_t A[256];           // bits of info j
     uint16_t S[256];           // sum over j of N[j][q]
@@ -90,15 +95,84 @@ __device__ __forceinline__ uint32_t warp_max(uint32_t v)
     return v;
 }
 
+// get_best_candidate's preference (include/CUDA_glutton_max.h:1196-1295): is candidate
+// (k, o) better than (k0, o0)?  order ~0 is "none".  Orders are distinct, so this is a
+// strict total order and any reduction tree finds the same best candidate.
+__device__ __forceinline__ bool better_candidate(unsigned long long k, uint32_t o, unsigned long long k0, uint32_t o0,
+                                                 bool last_level)
+{
+    if (o == ~0u) return false;
+    if (o0 == ~0u) return true;
+    return last_level ? o > o0 : (k > k0 || (k == k0 && o < o0));
+}
+
+// every lane ends with the warp's best (k, o)
+__device__ __forceinline__ void warp_best(unsigned long long& k, uint32_t& o, bool last_level)
+{
+    for (int d = 16; d; d >>= 1) {
+        const unsigned long long k2 = __shfl_xor_sync(kFull, k, d);
+        const uint32_t o2 = __shfl_xor_sync(kFull, o, d);
+        if (better_candidate(k2, o2, k, o, last_level)) {
+            k = k2;
+            o = o2;
+        }
+    }
+}
+
 __device__ __forceinline__ bool piece_available(const GmSmem& sm, uint32_t q)
 {
     return (sm.avail[q >> 5] >> (q & 31)) & 1u;
 }
 
-// Per-pass statistics of the current level (block-wide).
+// Six smallest (ASC) or largest of A[j]-N[j][q] over infos j in [j0, j1) for piece q,
+// as sorted lists of distinct keys (the info index in the low bits).
+template <bool ASC>
+__device__ __forceinline__ void extreme_six(const GmSmem& sm, uint32_t q, uint32_t j0, uint32_t j1, uint32_t* best,
+                                            uint32_t* sum)
+{
+    uint32_t s = 0;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) best[k] = ASC ? ~0u : 0u;
+    for (uint32_t j = j0; j < j1; ++j) {
+        const uint32_t n = sm.N[j][q];
+        s += n;
+        uint32_t v = ((sm.A[j] - n + (ASC ? 0u : 1u)) << 16) | j;
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            const uint32_t keep = ASC ? min(best[k], v) : max(best[k], v);
+            v = ASC ? max(best[k], v) : min(best[k], v);
+            best[k] = keep;
+        }
+    }
+    *sum = s;
+}
+
+// the first six of two sorted six-lists (ascending for ASC, else descending)
+template <bool ASC>
+__device__ __forceinline__ void merge_six(uint32_t* a, const uint32_t* b)
+{
+    uint32_t out[6];
+    int i = 0, k = 0;
+#pragma unroll
+    for (int o = 0; o < 6; ++o) {
+        const uint32_t x = a[i < 6 ? i : 5], y = b[k < 6 ? k : 5];
+        const bool take_a = k >= 6 || (i < 6 && (ASC ? x < y : x > y));
+        out[o] = take_a ? x : y;
+        i += take_a;
+        k += !take_a;
+    }
+#pragma unroll
+    for (int o = 0; o < 6; ++o) a[o] = out[o];
+}
+
+// Per-pass statistics of the current level (block-wide).  The per-piece scans run in
+// four groups of 256 threads (six smallest / six largest, each over one half of the
+// infos), merged afterwards; the lists are sets of distinct keys, so the halves and
+// the merge give the lists of one scan over all infos.
 __device__ void level_statistics(GmSmem& sm, uint32_t nb, uint32_t tid)
 {
     const uint32_t lane = tid & 31, warp = tid >> 5;
+    uint32_t asum = 0, aempty = 0;
     for (uint32_t j = warp; j < nb; j += kThreads / 32) {
         const uint32_t word = sm.X[j][lane];
         uint32_t packed0 = 0, packed1 = 0;
@@ -111,50 +185,36 @@ __device__ void level_statistics(GmSmem& sm, uint32_t nb, uint32_t tid)
         reinterpret_cast<uint32_t*>(sm.N[j])[2 * lane + 1] = packed1;
         const uint32_t a = warp_sum(__popc(word));
         if (lane == 0) sm.A[j] = static_cast<uint16_t>(a);
+        asum += a;
+        aempty |= a == 0;
+    }
+    if (lane == 0) {
+        sm.partA[warp] = asum;
+        sm.partE[warp] = aempty;
+    }
+    __syncthreads();
+    {
+        const uint32_t q = tid & 255u, group = tid >> 8, half = nb / 2;
+        const uint32_t j0 = (group & 1u) ? half : 0u, j1 = (group & 1u) ? nb : half;
+        uint32_t best[6], s;
+        if (group < 2) extreme_six<true>(sm, q, j0, j1, best, &s);
+        else extreme_six<false>(sm, q, j0, j1, best, &s);
+        uint32_t* dst = group == 0 ? sm.lo[q] : group == 1 ? sm.lo2[q] : group == 2 ? sm.hi[q] : sm.hi2[q];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) dst[k] = best[k];
+        if (group == 0) sm.S[q] = static_cast<uint16_t>(s);
+        if (group == 1) sm.S2[q] = static_cast<uint16_t>(s);
     }
     __syncthreads();
     if (tid < 256) {
-        // S[q] and the six smallest A[j]-N[j][q]
-        const uint32_t q = tid;
-        uint32_t s = 0;
-        uint32_t best[6] = {~0u, ~0u, ~0u, ~0u, ~0u, ~0u};
-        for (uint32_t j = 0; j < nb; ++j) {
-            const uint32_t n = sm.N[j][q];
-            s += n;
-            uint32_t v = ((sm.A[j] - n) << 16) | j;
-#pragma unroll
-            for (int k = 0; k < 6; ++k) {
-                const uint32_t lo = min(best[k], v), hi2 = max(best[k], v);
-                best[k] = lo;
-                v = hi2;
-            }
-        }
-        sm.S[q] = static_cast<uint16_t>(s);
-#pragma unroll
-        for (int k = 0; k < 6; ++k) sm.lo[q][k] = best[k];
+        merge_six<true>(sm.lo[tid], sm.lo2[tid]);
+        sm.S[tid] = static_cast<uint16_t>(sm.S[tid] + sm.S2[tid]);
     } else if (tid < 512) {
-        // the six largest, stored as (A[j]-N[j][q]+1) << 16 | j so that 0 marks an empty slot
-        const uint32_t q = tid - 256;
-        uint32_t best[6] = {0, 0, 0, 0, 0, 0};
-        for (uint32_t j = 0; j < nb; ++j) {
-            uint32_t v = ((sm.A[j] - sm.N[j][q] + 1u) << 16) | j;
-#pragma unroll
-            for (int k = 0; k < 6; ++k) {
-                const uint32_t big = max(best[k], v), small = min(best[k], v);
-                best[k] = big;
-                v = small;
-            }
-        }
-#pragma unroll
-        for (int k = 0; k < 6; ++k) sm.hi[q][k] = best[k];
+        merge_six<false>(sm.hi[tid - 256], sm.hi2[tid - 256]);
     } else if (tid < 544) {
-        uint32_t a = 0;
-        for (uint32_t j = tid - 512; j < nb; j += 32) a += sm.A[j];
-        a = warp_sum(a);
-        uint32_t empty = 0;
-        for (uint32_t j = tid - 512; j < nb; j += 32) empty |= sm.A[j] == 0;
-        empty = __any_sync(kFull, empty);
-        if (tid == 512) {
+        const uint32_t a = warp_sum(sm.partA[lane]);
+        const uint32_t empty = __any_sync(kFull, sm.partE[lane] != 0);
+        if (lane == 0) {
             sm.sumA = a;
             sm.any_empty = empty;
         }
@@ -501,28 +561,23 @@ __global__ void __launch_bounds__(kThreads, 1) gm_kernel(GmLaunch P)
                 sm.warp_trials[warp] = trials;
             }
             __syncthreads();
-            // this block's best (a strict total order: any reduction order gives the same result)
-            if (tid == 0) {
-                unsigned long long k0 = 0;
-                uint32_t o0 = ~0u;
-                unsigned long long tr = 0;
-                for (int w = 0; w < kThreads / 32; ++w) {
-                    tr += sm.warp_trials[w];
-                    const uint32_t o = sm.warp_order[w];
-                    if (o == ~0u) continue;
-                    const unsigned long long k = sm.warp_key[w];
-                    if (o0 == ~0u || (last_level ? o > o0 : (k > k0 || (k == k0 && o < o0)))) {
-                        k0 = k;
-                        o0 = o;
+            // this block's best, reduced by warp 0 (a strict total order: any reduction
+            // order gives the same result)
+            if (warp == 0) {
+                unsigned long long k0 = sm.warp_key[lane];
+                uint32_t o0 = sm.warp_order[lane];
+                warp_best(k0, o0, last_level);
+                unsigned long long tr = sm.warp_trials[lane];
+                for (int d = 16; d; d >>= 1) tr += __shfl_xor_sync(kFull, tr, d);
+                if (lane == 0) {
+                    if (GRID) {
+                        atomicAdd(&st->trials, tr);
+                        g->blk_key[buf][blockIdx.x] = k0;
+                        g->blk_order[buf][blockIdx.x] = o0;
+                    } else {
+                        st->trials += tr;
+                        sm.best_order = o0;
                     }
-                }
-                if (GRID) {
-                    atomicAdd(&st->trials, tr);
-                    g->blk_key[buf][blockIdx.x] = k0;
-                    g->blk_order[buf][blockIdx.x] = o0;
-                } else {
-                    st->trials += tr;
-                    sm.best_order = o0;
                 }
             }
             if (GRID) {
@@ -539,20 +594,24 @@ __global__ void __launch_bounds__(kThreads, 1) gm_kernel(GmLaunch P)
                         g->next_info[old] = 0;
                     }
                 }
-                if (tid == 0) {
-                    sm.any_invalid = *(volatile uint32_t*)&g->any_invalid[buf];
+                if (warp == 0) {
+                    // the blocks' bests, 32 at a time (the loads overlap instead of
+                    // waiting on L2 one block after another)
                     unsigned long long k0 = 0;
                     uint32_t o0 = ~0u;
-                    for (uint32_t b2 = 0; b2 < nblocks; ++b2) {
+                    for (uint32_t b2 = lane; b2 < nblocks; b2 += 32) {
                         const uint32_t o = *(volatile uint32_t*)&g->blk_order[buf][b2];
-                        if (o == ~0u) continue;
                         const unsigned long long k = *(volatile unsigned long long*)&g->blk_key[buf][b2];
-                        if (o0 == ~0u || (last_level ? o > o0 : (k > k0 || (k == k0 && o < o0)))) {
+                        if (better_candidate(k, o, k0, o0, last_level)) {
                             k0 = k;
                             o0 = o;
                         }
                     }
-                    sm.best_order = o0;
+                    warp_best(k0, o0, last_level);
+                    if (lane == 0) {
+                        sm.any_invalid = *(volatile uint32_t*)&g->any_invalid[buf];
+                        sm.best_order = o0;
+                    }
                 }
                 ++pass_no;
             }
