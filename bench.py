@@ -344,8 +344,8 @@ GM_WORKLOAD = (f"glutton max search of the seeded {GM_SIDE}x{GM_SIDE} puzzle ({G
 
 def glutton_reference_unit(native, handle, device):
     """The GPU's unit is its own trial count: validity passes over the whole level, which
-    evaluate more candidates than the reference's in-place sweep on the same trajectory.
-    The first pushes of the same search, whose reference-unit count the oracle recorded
+    evaluate a different number of candidates than the reference's in-place sweep on the
+    same trajectory.  The first pushes of the same search, whose reference-unit count the oracle recorded
     (tests/golden/glutton_16x16.json), give the rate in that unit."""
     golden = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tests", "golden", "glutton_16x16.json")
     if not os.path.exists(golden):
