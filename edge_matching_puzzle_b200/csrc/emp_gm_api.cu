@@ -299,3 +299,14 @@ extern "C" emp_status emp_glutton_max_noalloc(emp_puzzle puzzle, const emp_gm_co
     result->kernel_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
     return st.status == 1 ? EMP_INCOMPLETE : EMP_OK;
 }
+
+extern "C" emp_status emp_glutton_wide_situation(emp_puzzle puzzle, uint32_t* infos, uint64_t capacity_words)
+{
+    emp::clear_error();
+    if (!puzzle || !infos) return fail(EMP_ERR_INVALID, "emp_glutton_wide_situation: null argument");
+    const std::vector<uint32_t> cap = initial_capability(puzzle->model);
+    if (capacity_words < cap.size())
+        return fail(EMP_ERR_INVALID, "emp_glutton_wide_situation: capacity below 32 words per position");
+    std::memcpy(infos, cap.data(), cap.size() * sizeof(uint32_t));
+    return EMP_OK;
+}

@@ -5,7 +5,9 @@
 #include <chrono>
 #include <fstream>
 #include <cstring>
+#include <cstdio>
 #include <cstdlib>
+#include <iomanip>
 #include <sstream>
 
 namespace edge_matching_puzzle {
@@ -376,6 +378,58 @@ void feature_CUDA_glutton_max::run()
     m_out << "Max level : " << m_result.max_level << std::endl;
 }
 
+void print_position_info(std::ostream& out, const uint32_t* words)
+{
+    static const char kShort[4] = {'N', 'E', 'S', 'W'};
+    for (uint32_t w = 0; w < 32; ++w) {
+        uint32_t word = words[w];
+        if (!word) continue;
+        char hex[16];
+        std::snprintf(hex, sizeof(hex), "%08x", word);
+        out << "/" << std::string(8, '-') << " Word[" << std::setw(2) << w << "] : 0x" << hex << " "
+            << std::string(8, '-') << "\\" << std::endl;
+        for (uint32_t k = 0; k < 8; ++k) out << "|" << std::setw(4) << 8 * w + k;
+        out << "|" << std::endl;
+        for (uint32_t k = 0; k < 8; ++k) {
+            out << "|";
+            for (uint32_t o = 0; o < 4; ++o) out << (((word >> o) & 1u) ? kShort[o] : ' ');
+            word >>= 4;
+        }
+        out << "|" << std::endl;
+    }
+}
+
+feature_CUDA_glutton_wide::feature_CUDA_glutton_wide(const emp_piece_set& pieces, std::ostream& out)
+    : m_pieces(pieces), m_out(out)
+{
+}
+
+void feature_CUDA_glutton_wide::run()
+{
+    emp_puzzle_owner puzzle(m_pieces, nullptr);
+    const uint32_t n = m_pieces.width * m_pieces.height;
+    std::vector<uint32_t> infos(static_cast<size_t>(n) * 32);
+    const emp_status st = emp_glutton_wide_situation(puzzle.get(), infos.data(), infos.size());
+    if (st < 0) throw_abi("emp_glutton_wide_situation", st, __LINE__);
+    // the first situation: level 0, situation index 0, info index j holds position j
+    m_out << "Situation Level 0: " << std::endl;
+    m_out << "Situation Index 0: " << std::endl;
+    m_out << "===== Position index <-> Info index =====" << std::endl;
+    for (uint32_t j = 0; j < n; ++j) m_out << "Position[" << j << "] -> Index " << j << std::endl;
+    for (uint32_t j = 0; j < n; ++j) m_out << "Index[" << j << "] -> Position " << j << std::endl;
+    for (uint32_t j = 0; j < n; ++j) {
+        m_out << "Info[" << j << "]:" << std::endl;
+        print_position_info(m_out, &infos[static_cast<size_t>(j) * 32]);
+        m_out << std::endl;
+    }
+    for (uint32_t j = 0; j < n; ++j) {
+        m_out << "Theoric info[" << j << "]:" << std::endl;
+        print_position_info(m_out, &infos[static_cast<size_t>(j) * 32]);
+        m_out << std::endl;
+    }
+    m_out << std::endl;
+}
+
 feature_if& factory_feature::create_feature(const std::string& feature_name, const emp_piece_set& pieces,
                                             std::unique_ptr<emp_strategy_generator>& strategy,
                                             const feature_options& options, std::ostream& out,
@@ -394,6 +448,7 @@ feature_if& factory_feature::create_feature(const std::string& feature_name, con
         return *new feature_CUDA_backtracker(pieces, *strategy, options, out);
     }
     if (feature_name == "CUDA_glutton_max") return *new feature_CUDA_glutton_max(pieces, options, out);
+    if (feature_name == "CUDA_glutton_wide") return *new feature_CUDA_glutton_wide(pieces, out);
     throw emp_logic_error("Unsupported feature \"" + feature_name + "\"", __LINE__, __FILE__);
 }
 

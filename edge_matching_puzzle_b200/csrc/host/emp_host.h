@@ -193,9 +193,27 @@ class feature_CUDA_glutton_max : public feature_if {
     emp_gm_result m_result{};
 };
 
+// The reference's CUDA glutton wide (include/feature_CUDA_glutton_wide.h): its launcher
+// prepares the first situation of the search and prints it (src/CUDA_glutton_wide.cu:
+// 27-37, CUDA_glutton_situation::print in include/CUDA_glutton_situation.h:127-156).
+class feature_CUDA_glutton_wide : public feature_if {
+  public:
+    feature_CUDA_glutton_wide(const emp_piece_set& pieces, std::ostream& out = std::cout);
+    void run() override;
+
+  private:
+    const emp_piece_set& m_pieces;
+    std::ostream& m_out;
+};
+
+// One position info as the reference prints it (include/CUDA_piece_position_info2.h:
+// 315-352): per non-zero word its value, the eight piece ids and their orientations.
+void print_position_info(std::ostream& out, const uint32_t* words);
+
 class factory_feature {
   public:
-    // Creates the feature by name ("CUDA_backtracker", "CUDA_glutton_max").  The
+    // Creates the feature by name ("CUDA_backtracker", "CUDA_glutton_max",
+    // "CUDA_glutton_wide", "new_strategy", "new_text_strategy").  The
     // caller owns the returned object.  Other names throw "Unsupported feature".
     static feature_if& create_feature(const std::string& feature_name, const emp_piece_set& pieces,
                                       std::unique_ptr<emp_strategy_generator>& strategy,

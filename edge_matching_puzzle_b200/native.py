@@ -144,6 +144,7 @@ class GmResult(ctypes.Structure):
 # name -> (restype, argtypes); every symbol declared in include/emp_b200.h
 SIGNATURES = {
     "emp_abi_version": (ctypes.c_uint32, []),
+    "emp_glutton_wide_situation": (ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint32), ctypes.c_uint64]),
     "emp_last_error": (ctypes.c_char_p, []),
     "emp_generate_puzzle": (ctypes.c_int32, [ctypes.c_uint32] * 4 + [ctypes.c_uint64, u8p]),
     "emp_puzzle_create": (ctypes.c_int32, [ctypes.POINTER(PuzzleDesc), ctypes.POINTER(ctypes.c_void_p)]),
@@ -459,6 +460,13 @@ def glutton_max(puzzle: NativePuzzle, push_budget: int = 0, timeout_ms: int = 0,
     r = GmResult()
     check(load().emp_glutton_max(puzzle.handle, ctypes.byref(cfg), ctypes.byref(r)))
     return r
+
+
+def glutton_wide_situation(puzzle: NativePuzzle, n: int):
+    """emp_glutton_wide_situation: the n positions' level-0 infos, 32 words each."""
+    out = (ctypes.c_uint32 * (32 * n))()
+    check(load().emp_glutton_wide_situation(puzzle.handle, out, 32 * n))
+    return [list(out[32 * j:32 * j + 32]) for j in range(n)]
 
 
 def glutton_max_noalloc(puzzle: NativePuzzle, push_budget: int = 0, timeout_ms: int = 0,

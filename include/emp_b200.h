@@ -422,6 +422,17 @@ emp_status emp_glutton_max(emp_puzzle puzzle, const emp_gm_config *config, emp_g
  * kernel_ms is the host's wall time from the launch to the return of the result. */
 emp_status emp_glutton_max_noalloc(emp_puzzle puzzle, const emp_gm_config *config, emp_gm_result *result);
 
+/* ---------------- glutton wide (feature_CUDA_glutton_wide, include/feature_CUDA_glutton_wide.h) ----------------
+ * The reference's CUDA glutton wide prepares its first situation and prints it
+ * (src/CUDA_glutton_wide.cu:27-37; the search itself is not written there).  That
+ * situation is the level the glutton max search starts from: every position's info,
+ * with corner and border pieces in their forced orientation and centre pieces in all
+ * four (include/CUDA_common_glutton.h:150-211).  infos[32 * j + w] receives word w of
+ * position j's info, bit 4 * (piece % 8) + orientation of word piece / 8 (piece ids
+ * from 0), for the width * height positions; at level 0 info index j is position j.
+ * capacity_words must be at least 32 * width * height. */
+emp_status emp_glutton_wide_situation(emp_puzzle puzzle, uint32_t *infos, uint64_t capacity_words);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1076,9 +1076,10 @@ static void gm_apply(gm_state *g, uint32_t best)
     if (invalid) gm_pop(g);
 }
 
-int op_gm_run(op_puzzle *p, uint64_t budget, uint64_t push_budget, op_gm_result *out)
+/* The glutton search's first level: colour constraints and the initial capability of
+ * every position (also the situation CUDA glutton wide prints). */
+static gm_state *gm_setup(op_puzzle *p, uint64_t budget)
 {
-    memset(out, 0, sizeof(*out));
     gm_state *g = (gm_state *)calloc(1, sizeof(gm_state));
     g->p = p; g->size = p->n; g->n = p->n; g->budget = budget;
     uint32_t S = g->size;
@@ -1134,6 +1135,25 @@ int op_gm_run(op_puzzle *p, uint64_t budget, uint64_t push_budget, op_gm_result 
         g->position_index[pos] = pos;
         g->info_index[pos] = pos;
     }
+    return g;
+}
+
+/* CUDA glutton wide's situation (src/CUDA_glutton_wide.cu:27-37): level-0 infos of
+ * the n positions, 32 words each, info index = position index. */
+int op_gm_initial(op_puzzle *p, uint32_t *out)
+{
+    gm_state *g = gm_setup(p, 0);
+    for (uint32_t pos = 0; pos < p->n; ++pos) memcpy(out + 32 * (size_t)pos, gm_info(g, 0, pos), 32 * sizeof(uint32_t));
+    free(g->infos);
+    free(g->cc);
+    free(g);
+    return 0;
+}
+
+int op_gm_run(op_puzzle *p, uint64_t budget, uint64_t push_budget, op_gm_result *out)
+{
+    memset(out, 0, sizeof(*out));
+    gm_state *g = gm_setup(p, budget);
     /* kernel, CUDA_glutton_max.h:1522-1637 */
     int new_level = 1;
     uint32_t pop_index = 0;

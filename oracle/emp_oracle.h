@@ -133,6 +133,8 @@ typedef struct {
  * that many placements (trials + pushes), push_budget: after that many
  * pushes, checked at the top of each level (0: none). */
 int op_gm_run(op_puzzle *p, uint64_t budget, uint64_t push_budget, op_gm_result *out);
+/* the glutton search's first situation: out[32 * pos + w], n positions */
+int op_gm_initial(op_puzzle *p, uint32_t *out);
 
 /* The reference's variable-space CUDA backtracker (feature CUDA_backtracker,
  * src/CUDA_backtracker.cu:67-178 with include/system_equation_for_CUDA.h:70-173 and

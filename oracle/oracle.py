@@ -93,6 +93,7 @@ def lib():
         L.op_bt_estimate.restype = ctypes.c_double
         L.op_bt_estimate.argtypes = [vp, ctypes.POINTER(u32), u32, u64, ctypes.POINTER(ctypes.c_double)]
         L.op_gm_run.argtypes = [vp, u64, u64, ctypes.POINTER(GmResult)]
+        L.op_gm_initial.argtypes = [vp, ctypes.POINTER(u32)]
         _lib = L
     return _lib
 
@@ -222,3 +223,10 @@ class OraclePuzzle:
         r = GmResult()
         lib().op_gm_run(self._p, budget, push_budget, ctypes.byref(r))
         return r
+
+    def glutton_initial(self):
+        """The glutton search's first situation (what CUDA glutton wide prints): per
+        position its 32 info words."""
+        out = (ctypes.c_uint32 * (32 * self.n))()
+        lib().op_gm_initial(self._p, out)
+        return [list(out[32 * j:32 * j + 32]) for j in range(self.n)]

@@ -195,3 +195,43 @@ def test_backtracker_trace_mode_lines(cli, example, reference_vectors):
 def test_trace_mode_refuses_other_orders(cli, example):
     rc, out = run(cli, example("3_3"), "ressources", "CUDA_backtracker", "--trace=true", "--strategy=spiral")
     assert rc == 255 and "row-major" in out[-1], out
+
+
+def _reference_info_lines(words):
+    """CUDA_piece_position_info2's printer (include/CUDA_piece_position_info2.h:315-352),
+    restated here to check the host layer's C++ one."""
+    lines = []
+    for w, word in enumerate(words):
+        if not word:
+            continue
+        lines.append("/" + "-" * 8 + f" Word[{w:2d}] : 0x{word:08x} " + "-" * 8 + "\\")
+        lines.append("".join(f"|{8 * w + k:4d}" for k in range(8)) + "|")
+        cells = []
+        for k in range(8):
+            nib = (word >> (4 * k)) & 0xF
+            cells.append("|" + "".join("NESW"[o] if (nib >> o) & 1 else " " for o in range(4)))
+        lines.append("".join(cells) + "|")
+    return lines
+
+
+@pytest.mark.parametrize("name", ["3_3", "4_4", "5_5"])
+def test_glutton_wide_prints_the_first_situation(cli, example, reference_vectors, name):
+    """CUDA_glutton_wide: the reference's launcher prints the glutton's first situation
+    (src/CUDA_glutton_wide.cu:27-37, CUDA_glutton_situation::print); its infos equal
+    the oracle's first glutton level, which the glutton trajectory tests pin."""
+    from edge_matching_puzzle_b200 import native
+    from edge_matching_puzzle_b200.puzzle import Puzzle
+    from oracle.oracle import OraclePuzzle
+    pz = Puzzle.from_csv(reference_vectors["puzzles"][name])
+    n = pz.width * pz.height
+    want = OraclePuzzle(pz.width, pz.height, pz.colors).glutton_initial()
+    assert native.glutton_wide_situation(native.NativePuzzle(pz.width, pz.height, pz.colors), n) == want
+    rc, out = run(cli, example(name), "ressources", "CUDA_glutton_wide", "--enable_gui=false")
+    assert rc == 0
+    expect = ["Situation Level 0: ", "Situation Index 0: ", "===== Position index <-> Info index ====="]
+    expect += [f"Position[{j}] -> Index {j}" for j in range(n)] + [f"Index[{j}] -> Position {j}" for j in range(n)]
+    for title in ("Info", "Theoric info"):
+        for j in range(n):
+            expect += [f"{title}[{j}]:"] + _reference_info_lines(want[j]) + [""]
+    expect += [""]
+    assert out[1:] == expect
