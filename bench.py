@@ -584,6 +584,9 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
     ap.add_argument("--no-ttfs", action="store_true", help="skip the time-to-first-solution leg (plain vs learned)")
     ap.add_argument("--no-glutton", action="store_true", help="skip the 10 s glutton max leg of the default line")
+    ap.add_argument("--split-budget", type=int, default=0,
+                    help="DFS steps before a thread hands its remaining work back once a round's queue is empty "
+                         "(0: library default)")
     ap.add_argument("--stack-placement", type=int, default=0,
                     help="DFS stack: 0 library default, 1 shared 32-bit, 2 shared 16-bit, 3 global memory, 4 one DFS per warp")
     ap.add_argument("--host-loop", action="store_true",
@@ -641,7 +644,7 @@ def main():
     # of its own, so the rounds of one puzzle fill the GPU while another drains.
     graphs = not args.host_loop
     plans = [native.BtPlan([p], split_depth=DEPTH, device=local_rank, use_graph=int(graphs),
-                           stack_placement=args.stack_placement) for p in puzzles]
+                           stack_placement=args.stack_placement, split_budget=args.split_budget) for p in puzzles]
     counts = [pl.subtrees() for pl in plans]
     total_subtrees = sum(counts)
     flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.int32, device="cuda")
@@ -745,7 +748,7 @@ def main():
             t0 = time.perf_counter()
             hp = [native.NativePuzzle(WIDTH, HEIGHT, p.colors) for p in host_inputs]
             res = native.bt_count_batch(hp, split_depth=DEPTH, device=local_rank, sample_first=s,
-                                        sample_stride=SLICES)
+                                        sample_stride=SLICES, split_budget=args.split_budget)
             torch.cuda.synchronize()
             dt = time.perf_counter() - t0
             if i >= 1:

@@ -101,7 +101,7 @@ extern "C" emp_status emp_bt_autotune(const emp_puzzle* puzzles, uint32_t count,
             consider(c);
         }
     }
-    for (uint32_t budget : {512u, 2048u, 8192u, 32768u}) {
+    for (uint32_t budget : {64u, 256u, 512u, 2048u, 8192u}) {
         if (budget == best.split_budget) continue;
         emp_bt_config c = best;
         c.split_budget = budget;
