@@ -2,7 +2,7 @@
  * CPU oracle for edge_matching_puzzle_b200 -- TEST INFRASTRUCTURE ONLY.
  *
  * This is a plain-C restatement of the reference's CPU search code, used as
- * the bit-exact judge for the CUDA kernels.  Only the test-suite, the smoke
+ * the bit-exact checker of the CUDA kernels.  Only the test-suite, the smoke
  * check and the CPU-baseline leg of the benchmark may load it; the product
  * path (the CUDA library behind include/emp_b200.h) never calls it.
  *

@@ -1,6 +1,6 @@
 """GPU parity of the exhaustive backtracker against the CPU oracle (bit-exact counts).
 
-The CUDA path is reached through the C ABI (libemp_b200.so); the oracle is the judge.
+The CUDA path is reached through the C ABI (libemp_b200.so); the oracle is the checker.
 """
 from __future__ import annotations
 

@@ -1,6 +1,6 @@
 """The CPU oracle reproduces every golden vector the reference ships for this path.
 
-These pins are what makes the oracle a trustworthy judge for the CUDA kernels:
+These pins are what makes the oracle a trustworthy checker of the CUDA kernels:
   * tests/new_strategy_{3_3,4_4,5_5}: node and solution counts, the full "New max" trace
     and the results.bin dump, byte for byte (spiral order);
   * tests/CUDA_glutton_max_{3_3,4_4,5_5}: final boards of the glutton max search;
