@@ -485,10 +485,14 @@ emp_status create_plan(const emp_puzzle* puzzles, uint32_t count, const emp_bt_c
     pl->capacity = std::min<uint64_t>(pl->capacity, (uint64_t)1 << 23);
     CUDA_TRY(pl->rec_a.alloc(sizeof(uint32_t) * pl->rec_words * pl->capacity));
     CUDA_TRY(pl->rec_b.alloc(sizeof(uint32_t) * pl->rec_words * pl->capacity));
-    // default split budget: measured on a B200 over slices of four 8x8 workload puzzles,
-    // 2.68e10 placements/s at 2048 steps, 3.65e10 at 256, 3.79e10 at 64, 3.79e10 at 32
-    // (the round's tail is shared out sooner; rounds grow from about 20 to 29 per slice)
-    pl->budget = pl->cfg.split_budget ? pl->cfg.split_budget : 64u;
+    // default split budget.  Without a deadline the whole tree gets searched and a small
+    // budget shares each round's tail out sooner: measured on a B200 over slices of four
+    // 8x8 workload puzzles, 2.68e10 placements/s at 2048 steps, 3.65e10 at 256, 3.79e10
+    // at 64.  Under a deadline, instances that cannot finish would hand 64-step pieces
+    // back every round and bury the last records of the small ones (a batch of small
+    // puzzles and two 9x9 ones left small ones unfinished at 400 ms); 2048 keeps records
+    // whole longer, so the small instances finish first.
+    pl->budget = pl->cfg.split_budget ? pl->cfg.split_budget : (pl->cfg.timeout_ms ? 2048u : 64u);
     if (resume) {
         CUDA_TRY(pl->rec_init.reserve(sizeof(uint32_t) * resume_recs.size()));
         CUDA_TRY(cudaMemcpy(pl->rec_init.p, resume_recs.data(), sizeof(uint32_t) * resume_recs.size(),

@@ -110,7 +110,8 @@ typedef struct emp_bt_config {
     uint32_t keep_subtree_counts;/* 1: keep per-subtree counts for emp_bt_plan_subtree_counts */
     uint32_t split_budget;       /* once a round's queue is empty, a thread that spent this many
                                     DFS steps on its work record hands the rest back as new records
-                                    for the next round; 0 = default (64) */
+                                    for the next round; 0 = default (64 steps, or 2048 with
+                                    a timeout_ms deadline) */
     uint32_t sample_stride;      /* emp_bt_count[_batch]: count only subtrees sample_first,
                                     sample_first+sample_stride, ...; 0 = all subtrees */
     uint32_t sample_first;
