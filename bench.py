@@ -20,8 +20,9 @@ of the same subtrees: the reference's search is single-threaded and has no way t
 search one subtree, so the multi-threaded restatement is the CPU path timed.
 
 On one GPU the default line also carries ttfs (time to a first solution, plain order
-against the learned order) and glutton (a 10 s glutton max search of the 16x16 puzzle:
-placements/s, levels/s, best level, and the rate in the reference's trial unit).
+against the learned order), glutton (a 10 s glutton max search of the 16x16 puzzle:
+placements/s, levels/s, best level, and the rate in the reference's trial unit) and
+batch (one autotuned graph launch over the 4096 mixed instances with a 2 s deadline).
 """
 from __future__ import annotations
 
@@ -206,6 +207,52 @@ def _batch_cpu_sample(batch, threads, stride=16, node_limit=20_000_000):
     with cf.ThreadPoolExecutor(max_workers=threads) as ex:
         nodes = sum(ex.map(one, sample))
     return nodes, time.perf_counter() - t0, len(sample)
+
+
+def batch_leg(local_rank):
+    """The 4096 mixed instances for the default line: the autotuner's parameters, one
+    warm-up launch and one timed graph launch with the 2 s deadline."""
+    import torch
+    from edge_matching_puzzle_b200 import native
+    from edge_matching_puzzle_b200.puzzle import mixed_batch
+    batch = mixed_batch(BATCH_COUNT)
+    handles = [native.NativePuzzle(p.width, p.height, p.colors) for p in batch]
+    tune = native.bt_autotune(handles, trial_ms=200, use_graph=1, table_placement=1, device=local_rank)
+    cfg = native.config_dict(tune.best)
+    cfg.update(timeout_ms=BATCH_STEP_MS, use_graph=1, device=local_rank)
+    plan = native.BtPlan(handles, **cfg)
+    start_ev = torch.cuda.Event(enable_timing=True)
+    end_ev = torch.cuda.Event(enable_timing=True)
+    res = None
+    ms = 0.0
+    for i in range(2):
+        torch.cuda.synchronize()
+        start_ev.record()
+        plan.run(torch.cuda.current_stream().cuda_stream)
+        end_ev.record()
+        torch.cuda.synchronize()
+        res = plan.results()
+        ms = start_ev.elapsed_time(end_ev)
+    nodes = sum(r.nodes - r.expansion_nodes for r in res)
+    verified = {"checked": 0, "mismatched": 0}
+    golden_path = os.path.join(ROOT, "tests", "golden", "batch_counts.json")
+    if os.path.exists(golden_path):
+        with open(golden_path) as f:
+            golden = {r["instance"]: (r["nodes"], r["solutions"]) for r in json.load(f)["records"]}
+        for j, r in enumerate(res):
+            if r.status == native.EMP_OK and j in golden:
+                verified["checked"] += 1
+                verified["mismatched"] += int((r.nodes, r.solutions) != golden[j])
+    out = {"workload": BATCH_WORKLOAD, "placements_per_s": nodes / (ms / 1000.0) if ms else None, "launch_ms": ms,
+           "instances_complete": sum(1 for r in res if r.status == native.EMP_OK), "verified": verified,
+           "autotune": {"trials": tune.trials, "best_rate": tune.best_rate, "default_rate": tune.default_rate,
+                        "split_subtrees": cfg.get("split_subtrees"), "split_budget": cfg.get("split_budget"),
+                        "stack_placement": cfg.get("stack_placement"),
+                        "threads_per_block": cfg.get("threads_per_block")}}
+    plan.close()
+    for h in handles:
+        h.close()
+    return out
 
 
 def run_batch(args, rank, world, local_rank):
@@ -584,6 +631,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
     ap.add_argument("--no-ttfs", action="store_true", help="skip the time-to-first-solution leg (plain vs learned)")
     ap.add_argument("--no-glutton", action="store_true", help="skip the 10 s glutton max leg of the default line")
+    ap.add_argument("--no-batch", action="store_true", help="skip the 4096-instance batch leg of the default line")
     ap.add_argument("--split-budget", type=int, default=0,
                     help="DFS steps before a thread hands its remaining work back once a round's queue is empty "
                          "(0: library default)")
@@ -770,6 +818,12 @@ def main():
     glutton = None
     if rank == 0 and world == 1 and not args.no_glutton:
         glutton = glutton_leg(local_rank)
+    batch = None
+    if rank == 0 and world == 1 and not args.no_batch:
+        try:
+            batch = batch_leg(local_rank)
+        except Exception as e:  # the headline line must still print; the object says why it is missing
+            batch = {"error": f"{type(e).__name__}: {e}"[:300]}
 
     # ---------------- CPU baseline (oracle) and algorithmic work ----------------
     peaks, peak_kind = measured_peaks()
@@ -829,6 +883,7 @@ def main():
             "cpu_baseline": cpu,
             "ttfs": ttfs,
             "glutton": glutton,
+            "batch": batch,
             "dfs": {"rounds_per_step": rounds / args.steps, "launch": "host loop" if not graphs else
                     "one CUDA graph per puzzle slice (device-side round loop), 16 concurrent streams",
                     "busy_frac": busy / ms if ms and not graphs else None},
