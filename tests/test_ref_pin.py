@@ -5,7 +5,8 @@ tests/golden/ref_counts.json holds the counts that the reference's emp_strategy
 unmodified into oracle/_ref/ with the project's stand-ins for its missing libraries) gave
 on: the reference examples, the config-0 puzzles, the 24 random puzzles of the GPU tests,
 puzzles whose identical-piece masks clear other pieces' bits or fall outside a bitfield,
-400 instances of the mixed batch and resumed searches (--initial_situation).  Every one
+400 instances of the mixed batch, resumed searches (--initial_situation) and three whole
+8x8 workload seeds.  Every one
 of them has identical pieces except the reference examples, so this pins the
 HANDLE_IDENTICAL_PIECES path that every workload puzzle takes.  The GPU suite compares
 the CUDA path with the same file (tests/test_bt_gpu.py).
@@ -38,7 +39,7 @@ def test_identical_piece_path_is_covered():
     assert {r["group"] for r in identical} >= {"config0", "random", "quirk", "batch", "resume"}
 
 
-@pytest.mark.parametrize("rec", [r for r in RECORDS if r["group"] != "resume"], ids=lambda r: r["name"])
+@pytest.mark.parametrize("rec", [r for r in RECORDS if r["group"] not in ("resume", "8x8")], ids=lambda r: r["name"])
 def test_oracle_equals_reference(rec, tmp_path):
     pz = Puzzle.from_csv(rec["csv"])
     op = OraclePuzzle(pz.width, pz.height, pz.colors)
@@ -62,3 +63,17 @@ def test_oracle_resume_equals_reference(rec, tmp_path):
     assert (r.nodes, r.solutions) == (rec["nodes"], rec["solutions"])
     with open(res, "rb") as f:
         assert hashlib.sha256(f.read()).hexdigest() == rec["results_sha256"]
+
+
+def test_8x8_workload_seeds_equal_reference():
+    """Whole 8x8 workload seeds (4 border / 8 interior colours) counted by the reference's
+    own search: equal to the CPU oracle's counts in tests/golden/config_counts.json, which
+    the GPU suite checks the CUDA path against (test_8x8_full_count_against_cpu_golden).
+    The oracle needs minutes per seed, so this compares the two files."""
+    with open(os.path.join(ROOT, "tests", "golden", "config_counts.json")) as f:
+        oracle = {r["seed"]: (r["nodes"], r["solutions"]) for r in json.load(f)["records"] if r["config"] == "8x8"}
+    recs = [r for r in RECORDS if r["group"] == "8x8"]
+    assert len(recs) >= 3
+    for rec in recs:
+        assert rec["build"] == "identical"
+        assert (rec["nodes"], rec["solutions"]) == oracle[rec["seed"]], rec["name"]
