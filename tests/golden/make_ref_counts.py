@@ -21,7 +21,7 @@ drops such a write and counts it).  Cases:
   batch        instances of the 4096-instance mixed batch with small trees
   resume       set_initial_state (the --initial_situation parameter) from mid-board
                situations of random puzzles: the search resumes there and runs to its end
-  8x8 (--big)  whole counts of the smallest 8x8 workload seeds
+  8x8 (--big)  whole counts of 8x8 workload seeds (--big-seeds)
 
 The JSON is committed; the tests never run the reference.
 """
@@ -197,7 +197,10 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", required=True, help="root of the reference project (read-only)")
     ap.add_argument("--jobs", type=int, default=os.cpu_count() or 1)
-    ap.add_argument("--big", action="store_true", help="also count the smallest 8x8 workload seeds")
+    ap.add_argument("--big", action="store_true", help="also count whole 8x8 workload seeds")
+    ap.add_argument("--big-seeds", default="4,12,1",
+                    help="comma-separated 8x8 workload seeds for --big (the reference's search is single-threaded: "
+                         "2.9e7 placements/s per core, so a seed of 2e11 placements takes about two hours)")
     a = ap.parse_args()
     subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref", "REF=" + a.reference], check=True)
     cases = []
@@ -214,7 +217,7 @@ def main():
     cases += batch_cases()
     cases += resume_cases()
     if a.big:
-        for seed in (4, 12, 1):
+        for seed in (int(x) for x in a.big_seeds.split(",")):
             cases.append(dict(name=f"8x8_{seed}", group="8x8", csv=generate(8, 8, 4, 8, seed).to_csv(),
                               order="basic", seed=seed))
     records = []
