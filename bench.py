@@ -17,7 +17,9 @@ all rounds, result download inside the timed region).  The reference arm times t
 restatement of emp_strategy (oracle/emp_oracle.c, checked against the reference's own
 search built from its sources in oracle/_ref) on all host cores over a bounded sample
 of the same subtrees: the reference's search is single-threaded and has no way to
-search one subtree, so the multi-threaded restatement is the CPU path timed.
+search one subtree, so the multi-threaded restatement is the CPU path timed; its line
+carries reference_build, the reference's own search (oracle/_ref) and the restatement
+timed on one core each on the same whole puzzle.
 
 On one GPU the default line also carries ttfs (time to a first solution, plain order
 against the learned order), glutton (a 10 s glutton max search of the 16x16 puzzle:
@@ -594,6 +596,43 @@ def run_learned(args, rank, world, local_rank):
     print(json.dumps(out), flush=True)
 
 
+REF_CAL_INSTANCE = 2569  # a 7x7 instance of the mixed batch: 301 369 589 placements, 1 solution
+
+
+def reference_build_rate():
+    """The reference's own search (oracle/_ref, built from its sources) and the port on
+    one core each, on one whole puzzle: the reference's code per core next to the port
+    that this arm times.  The reference's search cannot take a sample of subtrees (it
+    runs from the root, or from an initial situation to the end of the tree)."""
+    from edge_matching_puzzle_b200.puzzle import mixed_batch
+    from oracle.oracle import OraclePuzzle
+    pz = mixed_batch(REF_CAL_INSTANCE + 1)[REF_CAL_INSTANCE]
+    op = OraclePuzzle(pz.width, pz.height, pz.colors)
+    binary = os.path.join(ROOT, "oracle", "_ref",
+                          "emp_ref_strategy_identical" if op.has_identical else "emp_ref_strategy_plain")
+    if not os.path.exists(binary):
+        return {"unavailable": "oracle/_ref is not built here (it is built where the reference tree is present)"}
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "puzzle.txt")
+        with open(path, "w") as f:
+            f.write(pz.to_csv())
+        t0 = time.perf_counter()
+        p = subprocess.run([binary, path, "basic", "/dev/null"], capture_output=True, text=True, cwd=d, timeout=300)
+        ref_s = time.perf_counter() - t0
+    if p.returncode != 0:
+        return {"unavailable": f"reference build exited {p.returncode}"}
+    grab = {k: int(line.split(":")[1]) for line in p.stdout.splitlines()
+            for k in ("Total situations explored", "Nb solutions") if line.startswith(k)}
+    t0 = time.perf_counter()
+    r, _ = op.run()
+    port_s = time.perf_counter() - t0
+    return {"puzzle": f"instance {REF_CAL_INSTANCE} of the mixed batch ({pz.width}x{pz.height})",
+            "placements": grab.get("Total situations explored"), "solutions": grab.get("Nb solutions"),
+            "reference_per_core": grab.get("Total situations explored", 0) / ref_s, "port_per_core": r.nodes / port_s,
+            "port_over_reference": ref_s / port_s,
+            "same_counts": (r.nodes, r.solutions) == (grab.get("Total situations explored"), grab.get("Nb solutions"))}
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -617,6 +656,10 @@ def run_reference(args, rank, world):
                                    f"oracle restatement of emp_strategy, one pthread per core"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    try:
+        out["reference_build"] = reference_build_rate()
+    except Exception as e:  # the arm's line must still print
+        out["reference_build"] = {"unavailable": f"{type(e).__name__}: {e}"[:200]}
     print(json.dumps(out), flush=True)
 
 
